@@ -1,0 +1,355 @@
+"""Benchmark: DOF-updates/s of the fused FP64 DGSEM tendency + RK3 path.
+
+Workload (one "step"): CompressibleIdealGas2D on a periodic 128x128 quad mesh
+of [0,1]^2 with interior nodes perturbed by 0.02*h*sin(2 pi x)sin(2 pi y),
+N = 7 Legendre-Gauss (4 conservative variables, 4,194,304 DOF), gamma = 1.4,
+rho = 1 + 0.1 sin(2 pi x) sin(2 pi y), (u, v) = (0.5, 0.3), p = 1, naive LLF
+flux, Williamson RK3 at CFL 0.5 (dt from CovariantArcMin), 200 RK3 steps:
+one full solve.  Inputs are seeded synthetic fields of this shape (the
+reference ships no data for it).
+
+Reported (one JSON line on rank 0):
+  value     DOF-updates/s with the state resident in HBM, device-timed with
+            CUDA events on the engine's stream, L2 flushed before every solve
+  e2e       the same metric through the public API with host buffers: each
+            step copies the initial state host->device from pinned memory,
+            runs the solve, and copies the final state back
+  roofline  algorithmic bytes per fused-stage launch / measured launch time
+  cpu_baseline  the CPU oracle (C++ restatement of the reference CPU path,
+            OpenMP over elements) on a bounded sample of the same workload
+
+``--impl reference`` times the reference algorithm's CPU implementation (the
+oracle port; the Fortran reference cannot be built in this image) on the same
+workload, metric and unit.  Multi-GPU: the path runs as independent replicas
+(one per rank, no data-path collective); value = all ranks' DOF-updates over
+the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, N, STEPS_PER_SOLVE, CFL = 128, 7, 200, 0.5
+NVAR, P = 4, N + 1
+NEL = NX * NX
+DOF = NVAR * P * P * NEL
+GAMMA = 1.4
+WORKLOAD = (f"CompressibleIdealGas2D periodic {NX}x{NX} perturbed(0.02h) N={N} Gauss, FP64, naive LLF, "
+            f"Williamson RK3 CFL {CFL}, {STEPS_PER_SOLVE} steps per solve")
+
+
+def algorithmic_bytes_per_element_stage():
+    """Bytes one element must move per RK stage (8-byte words):
+    state read+write and RK register read+write (4*nVar*P^2), own 9-field
+    traces written + neighbour traces read (2*4*9*P), metric terms dsdx(4)+J(1)
+    per node and nHat(2)+nScale(1) per face node, 80 B of sideInfo."""
+    w = 8
+    return w * (4 * NVAR * P * P + 2 * 4 * 9 * P) + w * (5 * P * P + 12 * P) + 80
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def recorded_traffic():
+    """DRAM bytes per fused-stage launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "fused_stage_cig_c2.txt")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def initial_state(x):
+    X, Y = x[..., 0], x[..., 1]  # x: (nEl, 1, P, P, 2) device tensor
+    rho = 1.0 + 0.1 * (2 * np.pi * X).sin() * (2 * np.pi * Y).sin()
+    import torch
+    q = torch.empty((NEL, 4, P, P), device=x.device, dtype=torch.float64)
+    q[:, 0] = (rho * 0.5)[:, 0]
+    q[:, 1] = (rho * 0.3)[:, 0]
+    q[:, 2] = rho[:, 0]
+    q[:, 3] = (1.0 / (GAMMA - 1.0) + 0.5 * rho * (0.5 ** 2 + 0.3 ** 2))[:, 0]
+    return q
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.proc = index, None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(seconds=12.0, max_steps=STEPS_PER_SOLVE):
+    """The CPU oracle on the full mesh, stepping until `seconds` of work."""
+    from oracle import build as obuild
+    obuild.build()
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    O.set_threads(cores, fast=True)
+    m = O.Mesh(NX, NX, periodic=(True, True), amp=0.02)
+    mod = O.Model(O.CIG, N, m, fast=True)
+    g = O.Geometry(N, m)
+    X, Y = g.x[0, :, :, 0, :], g.x[1, :, :, 0, :]
+    q = np.zeros((P, P, 4, NEL), order="F")
+    rho = 1 + 0.1 * np.sin(2 * np.pi * X) * np.sin(2 * np.pi * Y)
+    q[:, :, 0], q[:, :, 1], q[:, :, 2] = rho * 0.5, rho * 0.3, rho
+    q[:, :, 3] = 1 / (GAMMA - 1) + 0.5 * rho * 0.34
+    mod.set("solution", q)
+    dt = 1e-4
+    mod.rk3(1, dt)  # warm-up
+    steps, t0 = 0, time.perf_counter()
+    while steps < max_steps and time.perf_counter() - t0 < seconds:
+        mod.rk3(1, dt)
+        steps += 1
+    el = time.perf_counter() - t0
+    return {"value": DOF * steps / el, "unit": "DOF-updates/s", "cores": cores, "kind": "port",
+            "sample": f"{steps} RK3 steps of the full {NX}x{NX} N={N} mesh ({steps}/{STEPS_PER_SOLVE} of a solve), "
+                      f"{el:.1f} s, C++ restatement of the reference CPU branches, OpenMP over elements"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import build as obuild
+    obuild.build()
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    O.set_threads(cores, fast=True)
+    m = O.Mesh(NX, NX, periodic=(True, True), amp=0.02)
+    mod = O.Model(O.CIG, N, m, fast=True)
+    g = O.Geometry(N, m)
+    X, Y = g.x[0, :, :, 0, :], g.x[1, :, :, 0, :]
+    q = np.zeros((P, P, 4, NEL), order="F")
+    rho = 1 + 0.1 * np.sin(2 * np.pi * X) * np.sin(2 * np.pi * Y)
+    q[:, :, 0], q[:, :, 1], q[:, :, 2] = rho * 0.5, rho * 0.3, rho
+    q[:, :, 3] = 1 / (GAMMA - 1) + 0.5 * rho * 0.34
+    mod.set("solution", q)
+    dt = 1e-4
+    for _ in range(args.warmup):
+        mod.rk3(1, dt)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        mod.rk3(1, dt)
+    el = time.perf_counter() - t0
+    v = DOF * args.steps / el
+    sample = (f"each step = 1 RK3 step of the full {NX}x{NX} N={N} mesh (1/{STEPS_PER_SOLVE} of a solve); "
+              f"C++ restatement of the reference CPU path (the Fortran reference needs gfortran, hipfort, MPI and "
+              f"HDF5, none of which exist in this image)")
+    print(json.dumps({
+        "impl": "reference", "metric": "DOF-updates/s", "value": v, "unit": "DOF-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "elements": NEL, "dof": DOF, "parallelism": "replicas"},
+        "cpu_baseline": {"value": v, "unit": "DOF-updates/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_engine(args, rank, world, local_rank):
+    import torch
+    import self_b200 as S
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.Stream(device=dev)
+    interp = S.Lagrange(N, S.GAUSS, N, S.UNIFORM)
+    mesh = S.Mesh2D(NX, NX, periodic=(True, True), perturbation=0.02)
+    geo = S.SEMQuad(interp, mesh)
+    model = S.CompressibleIdealGas2D(mesh, geo, stream=stream.cuda_stream)
+    q0 = initial_state(geo.x)
+    torch.cuda.synchronize()
+    # CFL time step: dt = CFL * ArcMin / max(|u| + c)
+    c = (GAMMA * 1.0 / (q0[:, 2].min())).sqrt().item()
+    dt = CFL * geo.CovariantArcMin() / (np.hypot(0.5, 0.3) + c)
+    flush = torch.empty(64 * 1024 * 1024, device=dev, dtype=torch.float32)  # 256 MB > 126 MB L2
+
+    def solve():
+        model.SetSolution(q0)
+        model.workSol.zero_()
+        model.ForwardStep(STEPS_PER_SOLVE, dt)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            solve()
+    stream.synchronize()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    launches0 = model.LaunchCount()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    try:
+        smi_id = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        smi_id = str(local_rank)
+    clocks = Clocks(smi_id)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with clocks, torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(stream)
+            solve()
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    launches = model.LaunchCount() - launches0  # fused-stage launches (plus one trace prologue per solve)
+    clk = clocks.summary()
+    t_max = ms
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = world * DOF * STEPS_PER_SOLVE * args.steps / (t_max / 1e3)
+    stage_ms = ms / (args.steps * 3 * STEPS_PER_SOLVE)
+    per_launch = algorithmic_bytes_per_element_stage() * NEL
+    achieved = per_launch / (stage_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = recorded_traffic()
+
+    # ---- end to end through the public API with host buffers
+    host_q = torch.empty(q0.shape, dtype=torch.float64, pin_memory=True)
+    host_q.copy_(q0.cpu())
+    host_out = torch.empty_like(host_q).pin_memory()
+    with torch.cuda.stream(stream):
+        for _ in range(max(1, args.warmup // 2)):
+            model.solution.copy_(host_q, non_blocking=True)
+            model.workSol.zero_()
+            S.lib().selfgpu_model2d_invalidate(model._h)
+            model.ForwardStep(STEPS_PER_SOLVE, dt)
+            host_out.copy_(model.solution, non_blocking=True)
+        stream.synchronize()
+        if dist:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            model.solution.copy_(host_q, non_blocking=True)
+            model.workSol.zero_()
+            S.lib().selfgpu_model2d_invalidate(model._h)
+            model.ForwardStep(STEPS_PER_SOLVE, dt)
+            host_out.copy_(model.solution, non_blocking=True)
+        e1.record(stream)
+        stream.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = world * DOF * STEPS_PER_SOLVE * args.steps / (e2e_ms / 1e3)
+    model.CheckFinite()
+
+    if rank != 0:
+        return
+    line = {
+        "metric": "DOF-updates/s", "value": value, "unit": "DOF-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "elements": NEL, "dof": DOF, "rk3_steps_per_step": STEPS_PER_SOLVE,
+                   "dt": dt, "parallelism": "replicas" if world > 1 else "single-gpu",
+                   "l2": "flushed (256 MB write) before every timed solve; per-stage working set ~150 MB > L2"},
+        "e2e": {"value": e2e, "unit": "DOF-updates/s", "h2d_bytes_per_step": int(host_q.numel() * 8),
+                "d2h_bytes_per_step": int(host_out.numel() * 8)},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_kind,
+                     "bytes_per_launch": per_launch, "launch_ms": stage_ms,
+                     "kernel": "k_fused_stage<8,PhysCIG,double> (one RK stage over all elements)"},
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="selfgpu", choices=["selfgpu", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local_rank)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_engine(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,298 @@
+/* selfgpu.h -- C ABI of libselfgpu, the B200 (sm_100a) DGSEM tendency engine
+ * for SELF's 2-D Model2D path.
+ *
+ * Two groups of entry points:
+ *
+ *  1. Drop-in replacements for SELF's HIP wrappers.  Same symbol names, same
+ *     argument lists and the same "pointer to device pointer" convention that
+ *     SELF's Fortran interfaces produce (TYPE(c_ptr) without VALUE arrives as
+ *     real**, INTEGER(C_INT),VALUE as int).  `real` is double: these are the
+ *     FP64 build (-DDOUBLE_PRECISION) of the reference.  Like the reference
+ *     they return void, launch on the legacy default stream and do not
+ *     synchronise; a launch failure is recorded and can be read with
+ *     selfgpu_last_error().  Layouts are SELF's Fortran column-major layouts
+ *     (src/hip/SELF_HIP_Macros.h:20-38 of the reference).
+ *
+ *  2. Fused entry points (selfgpu_*) that return an int status
+ *     (SELFGPU_OK == 0).  They run a whole CalculateTendency or whole
+ *     Williamson RK3 steps of LinearShallowWater, ShallowWater or
+ *     CompressibleIdealGas2D as one kernel per RK stage, on buffers that the
+ *     caller owns (the Fortran hfReal device arrays); only the engine's own
+ *     face-trace cache is allocated by the library, inside the handle.
+ *
+ * Every reference citation below is file:line inside the SELF repository.
+ */
+#ifndef SELFGPU_H
+#define SELFGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- constants */
+/* quadrature ids, src/SELF_Constants.f90:78-84 */
+#define SELFGPU_GAUSS 1
+#define SELFGPU_GAUSS_LOBATTO 2
+#define SELFGPU_UNIFORM 5
+/* boundary condition ids, src/hip/SELF_HIP_Macros.h:40-49 */
+#define SELFGPU_BC_PRESCRIBED 100
+#define SELFGPU_BC_RADIATION 101
+#define SELFGPU_BC_NONORMALFLOW 102
+/* models */
+#define SELFGPU_MODEL_LSW 1 /* LinearShallowWater, src/models/SELF_LinearShallowWater.f90 */
+#define SELFGPU_MODEL_SW 2  /* ShallowWater,       src/models/SELF_ShallowWater.f90 */
+#define SELFGPU_MODEL_CIG 3 /* CompressibleIdealGas2D, src/models/SELF_CompressibleIdealGas2D.f90 */
+/* arithmetic forms of the fused path */
+#define SELFGPU_FP64 0       /* plain FP64 (parity form) */
+#define SELFGPU_FP32_BULK 1  /* FP32 flux/divergence, FP64 metrics/sources/RK accumulation */
+/* largest polynomial degree the fused kernels are instantiated for */
+#define SELFGPU_MAX_N 7
+/* status codes */
+#define SELFGPU_OK 0
+#define SELFGPU_ERR_ARG 1      /* bad argument (null pointer, size, degree, model) */
+#define SELFGPU_ERR_MESH 2     /* malformed sideInfo rejected before launch */
+#define SELFGPU_ERR_CUDA 3     /* CUDA launch or runtime error */
+#define SELFGPU_ERR_STATE 4    /* handle not fully bound */
+#define SELFGPU_ERR_NONFINITE 5/* NaN/Inf found by selfgpu_model2d_check_finite */
+#define SELFGPU_ERR_TIMEOUT 6  /* a bounded device wait ran out */
+
+/* Message for the calling thread's most recent error ("" when none). */
+const char* selfgpu_last_error(void);
+
+/* ====================================================== 1. drop-in wrappers */
+
+/* -- Lagrange: src/SELF_Lagrange.f90 interfaces, src/hip/SELF_Lagrange.cpp -- */
+/* replaces ScalarGridInterp_2D_gpu_wrapper, SELF_Lagrange.cpp:107 */
+void ScalarGridInterp_2D_gpu_wrapper(double** iMatrix, double** f, double** fInterp, int N, int M, int nVar,
+                                     int nEl);
+/* replaces VectorGridInterp_2D_gpu_wrapper, SELF_Lagrange.cpp:140 */
+void VectorGridInterp_2D_gpu_wrapper(double** iMatrix, double** f, double** fInterp, int N, int M, int nVar,
+                                     int nEl);
+/* replaces ScalarBoundaryInterp_2D_gpu_wrapper, SELF_Lagrange.cpp:395 */
+void ScalarBoundaryInterp_2D_gpu_wrapper(double** bMatrix, double** f, double** fBound, int N, int nVar,
+                                         int nEl);
+/* replaces VectorBoundaryInterp_2D_gpu_wrapper, SELF_Lagrange.cpp:424 */
+void VectorBoundaryInterp_2D_gpu_wrapper(double** bMatrix, double** f, double** fBound, int N, int nVar,
+                                         int nEl);
+/* replaces TensorBoundaryInterp_2D_gpu_wrapper, SELF_Lagrange.cpp:483 */
+void TensorBoundaryInterp_2D_gpu_wrapper(double** bMatrix, double** f, double** fBound, int N, int nVar,
+                                         int nEl);
+/* replaces VectorGradient_2D_gpu_wrapper, SELF_Lagrange.cpp:730 */
+void VectorGradient_2D_gpu_wrapper(double** dMatrix, double** f, double** df, int N, int nVar, int nEl);
+/* replaces VectorDGDivergence_2D_gpu_wrapper, SELF_Lagrange.cpp:827 */
+void VectorDGDivergence_2D_gpu_wrapper(double** dgMatrix, double** bMatrix, double** qWeights, double** f,
+                                       double** bf, double** df, int N, int nVar, int nEl);
+
+/* -- Data / Geometry: src/hip/SELF_Data.cpp, src/hip/SELF_Geometry.cpp -- */
+/* replaces Determinant_Tensor2D_gpu_wrapper, SELF_Data.cpp:74 */
+void Determinant_Tensor2D_gpu_wrapper(double** tensor, double** detTensor, int N, int nVar, int nEl);
+/* replaces CalculateContravariantBasis_SEMQuad_gpu_wrapper, SELF_Geometry.cpp:96 */
+void CalculateContravariantBasis_SEMQuad_gpu_wrapper(double** dxds, double** dsdx, int N, int nEl);
+/* replaces AdjustBoundaryContravariantBasis_SEMQuad_gpu_wrapper, SELF_Geometry.cpp:123 */
+void AdjustBoundaryContravariantBasis_SEMQuad_gpu_wrapper(double** dsdx, double** J, int N, int nEl);
+
+/* -- MappedData: src/SELF_MappedData.f90:162-600, src/hip/SELF_MappedData.cpp -- */
+/* replaces GradientBR_MappedScalar2D_gpu_wrapper, SELF_MappedData.cpp:164 */
+void GradientBR_MappedScalar2D_gpu_wrapper(double** scalar, double** avgBoundary, double** dsdx, double** jacobian,
+                                           double** nHat, double** nScale, double** gradF, double** dgMatrix,
+                                           double** bMatrix, double** qWeights, int N, int nVar, int nEl);
+/* replaces GradientSF_MappedScalar2D_gpu_wrapper, SELF_MappedData.cpp:203 */
+void GradientSF_MappedScalar2D_gpu_wrapper(double** scalar, double** dsdx, double** jacobian, double** gradF,
+                                           double** dMatrix, int N, int nVar, int nEl);
+/* replaces JacobianWeight_MappedScalar2D_gpu_wrapper, SELF_MappedData.cpp:223 */
+void JacobianWeight_MappedScalar2D_gpu_wrapper(double** scalar, double** jacobian, int N, int nVar, int nEl);
+/* replaces ContravariantProjection_MappedVector2D_gpu_wrapper, SELF_MappedData.cpp:422 */
+void ContravariantProjection_MappedVector2D_gpu_wrapper(double** vector, double** dsdx, int N, int nVar, int nEl);
+/* replaces JacobianWeight_MappedVector2D_gpu_wrapper, SELF_MappedData.cpp:466 */
+void JacobianWeight_MappedVector2D_gpu_wrapper(double** vector, double** jacobian, int N, int nVar, int nEl);
+/* replaces SideExchange_MappedScalar2D_gpu_wrapper, SELF_MappedData.cpp:943 */
+void SideExchange_MappedScalar2D_gpu_wrapper(double** extBoundary, double** boundary, int** sideInfo,
+                                             int** elemToRank, int rankId, int offset, int N, int nVar, int nEl);
+/* replaces SideExchange_MappedVector2D_gpu_wrapper, SELF_MappedData.cpp:982 */
+void SideExchange_MappedVector2D_gpu_wrapper(double** extBoundary, double** boundary, int** sideInfo,
+                                             int** elemToRank, int rankId, int offset, int N, int nVar, int nEl);
+/* replaces BassiRebaySides_MappedScalar2D_gpu_wrapper, SELF_MappedData.cpp:1255 */
+void BassiRebaySides_MappedScalar2D_gpu_wrapper(double** avgBoundary, double** boundary, double** extBoundary,
+                                                int N, int nVar, int nEl);
+
+/* -- Model2D: src/SELF_Model2D.f90:73-138, src/hip/SELF_Model2D.cpp -- */
+/* replaces UpdateGRK_Model2D_gpu_wrapper, SELF_Model2D.cpp:153 */
+void UpdateGRK_Model2D_gpu_wrapper(double** grk, double** solution, double** dSdt, double rk_a, double rk_g,
+                                   double dt, int nWork, int N, int nVar, int nEl);
+/* replaces UpdateSolution_Model2D_gpu_wrapper, SELF_Model2D.cpp:172 */
+void UpdateSolution_Model2D_gpu_wrapper(double** solution, double** dSdt, double dt, int N, int nVar, int nEl);
+/* replaces CalculateDSDt_Model2D_gpu_wrapper, SELF_Model2D.cpp:192 */
+void CalculateDSDt_Model2D_gpu_wrapper(double** fluxDivergence, double** source, double** dSdt, int N, int nVar,
+                                       int nEl);
+
+/* -- LinearShallowWater: src/models/SELF_LinearShallowWater.f90:53-97, models/hip/SELF_LinearShallowWater.cpp -- */
+/* replaces SetBoundaryCondition_LinearShallowWater_gpu_wrapper, SELF_LinearShallowWater.cpp:48
+ * (follows the CPU reflection (n_y^2 - n_x^2), SELF_LinearShallowWater.f90:336) */
+void SetBoundaryCondition_LinearShallowWater_gpu_wrapper(double** solution, double** extBoundary, double** nHat,
+                                                         int** sideInfo, int N, int nVar, int nEl);
+/* replaces Source_LinearShallowWater_gpu_wrapper, SELF_LinearShallowWater.cpp:73 */
+void Source_LinearShallowWater_gpu_wrapper(double** source, double** solution, double** f, int N, int nVar, int nEl);
+/* replaces Flux_LinearShallowWater_gpu_wrapper, SELF_LinearShallowWater.cpp:102 */
+void Flux_LinearShallowWater_gpu_wrapper(double** flux, double** solution, double** H, double g, int N, int nVar,
+                                         int nEl);
+/* replaces RiemannSolver_LinearShallowWater_gpu_wrapper, SELF_LinearShallowWater.cpp:141 */
+void RiemannSolver_LinearShallowWater_gpu_wrapper(double** flux, double** solution, double** extBoundary, double** H,
+                                                  double** nHat, double** nScale, double g, int N, int nVar,
+                                                  int nEl);
+
+/* -- ShallowWater (nonlinear).  The reference has no device path for this model
+ * (its GPU calls are commented out, src/models/SELF_ShallowWater.f90:293-303,
+ * :351-360, :392-399, :463-475); these follow the Fortran interfaces those
+ * comments name, extended with the fields the CPU path reads. -- */
+/* CPU SetBoundaryCondition_ShallowWater, SELF_ShallowWater.f90:284-343 */
+void SetBoundaryCondition_ShallowWater_gpu_wrapper(double** solution, double** extBoundary, double** topoBoundary,
+                                                   double** nHat, int** sideInfo, int N, int nVar, int nEl);
+/* CPU Source_ShallowWater, SELF_ShallowWater.f90:345-384 */
+void Source_ShallowWater_gpu_wrapper(double** source, double** solution, double** gradH, double fCori, double g,
+                                     int N, int nVar, int nEl);
+/* CPU Flux_ShallowWater, SELF_ShallowWater.f90:386-449 (velocity = PreTendency output) */
+void Flux_ShallowWater_gpu_wrapper(double** flux, double** solution, double** velocity, double g, int N, int nVar,
+                                   int nEl);
+/* CPU RiemannSolver_ShallowWater, SELF_ShallowWater.f90:451-529 */
+void RiemannSolver_ShallowWater_gpu_wrapper(double** flux, double** solution, double** extBoundary,
+                                            double** velocity, double** extVelocity, double** nHat,
+                                            double** nScale, double g, int N, int nVar, int nEl);
+/* CPU PreTendency_ShallowWater velocity step, SELF_ShallowWater.f90:190-239 (without the exchange) */
+void PreTendency_ShallowWater_gpu_wrapper(double** solution, double** solutionBoundary, double** velocity,
+                                          double** velocityBoundary, int N, int nVar, int nEl);
+
+/* -- CompressibleIdealGas2D: src/models/SELF_CompressibleIdealGas2D.f90:149-257,
+ *    models/hip/SELF_CompressibleIdealGas2D.cpp.  These follow the CPU
+ *    branches (hazards: FP64 sound speed, rhoKE = 0.5(rhoU u + rhoV v)). -- */
+/* replaces Source_CompressibleIdealGas2D_gpu_wrapper, SELF_CompressibleIdealGas2D.cpp:28.  The
+ * reference wrapper receives no drag field; like the reference device kernel
+ * this one applies gravity only.  The fused path applies gravity and drag. */
+void Source_CompressibleIdealGas2D_gpu_wrapper(double** source, double** solution, double** environmentalsGradient,
+                                               int N, int nVar, int nEl);
+/* replaces Flux_CompressibleIdealGas2D_gpu_wrapper, SELF_CompressibleIdealGas2D.cpp:95 */
+void Flux_CompressibleIdealGas2D_gpu_wrapper(double** flux, double** solution, double** primitive, int N, int nVar,
+                                             int nEl);
+/* replaces NaiveLLF_CompressibleIdealGas2D_gpu_wrapper, SELF_CompressibleIdealGas2D.cpp:190 */
+void NaiveLLF_CompressibleIdealGas2D_gpu_wrapper(double** flux, double** solution, double** extSolution,
+                                                 double** primitive, double** extPrimitive, double** diagnostics,
+                                                 double** extDiagnostics, double** nHat, double** nScale, int N,
+                                                 int nVar, int nDiag, int nEl);
+/* replaces SetBoundaryCondition_CompressibleIdealGas2D_gpu_wrapper, SELF_CompressibleIdealGas2D.cpp:286 */
+void SetBoundaryCondition_CompressibleIdealGas2D_gpu_wrapper(
+    double** solution, double** extSolution, double** prescribedSolution, double** primitive, double** extPrimitive,
+    double** prescribedPrimitive, double** diagnostics, double** extDiagnostics, double** prescribedDiagnostics,
+    double** nHat, int** sideInfo, int N, int nVar, int nDiag, int nEl);
+/* replaces CalculateDiagnostics_CompressibleIdealGas2D_gpu_wrapper, SELF_CompressibleIdealGas2D.cpp:363 */
+void CalculateDiagnostics_CompressibleIdealGas2D_gpu_wrapper(double** solution, double** diagnostics,
+                                                             double expansionFactor, double R, int N, int nVar,
+                                                             int nDiag, int nEl);
+/* replaces ConservativeToPrimitive_CompressibleIdealGas2D_gpu_wrapper, SELF_CompressibleIdealGas2D.cpp:402 */
+void ConservativeToPrimitive_CompressibleIdealGas2D_gpu_wrapper(double** solution, double** primitive,
+                                                                double expansionFactor, int N, int nVar, int nEl);
+/* replaces ConservativeToEntropy_CompressibleIdealGas2D_gpu_wrapper, SELF_CompressibleIdealGas2D.cpp:442 */
+void ConservativeToEntropy_CompressibleIdealGas2D_gpu_wrapper(double** solution, double** entropy,
+                                                              double expansionFactor, int N, int nVar, int nEl);
+
+/* ========================================================= 2. host set-up */
+
+/* Nodes and weights, src/SELF_Quadrature.f90:59-116 (LegendreQuadrature). */
+int selfgpu_legendre_quadrature(int N, int type, double* nodes, double* weights);
+
+/* Lagrange%Init host arrays, src/SELF_Lagrange.f90:521-615.  Layouts:
+ * iMatrix(0:N,0:M), dMatrix(0:N,0:N), dgMatrix(0:N,0:N), bMatrix(0:N,0:1). */
+int selfgpu_lagrange_init(int N, int controlNodeType, int M, int targetNodeType, double* controlPoints,
+                          double* targetPoints, double* bWeights, double* qWeights, double* iMatrix,
+                          double* dMatrix, double* dgMatrix, double* bMatrix);
+
+/* Structured nx*ny quadrilateral mesh on [x0,x1]x[y0,y1] (nGeo = 1) in the
+ * layout Mesh2D%Read_HOPr produces (src/SELF_Mesh.f90:852-1016):
+ * nodeCoords(1:2,0:1,0:1,nEl), globalNodeIDs(0:1,0:1,nEl), sideInfo(1:5,1:4,nEl).
+ * Periodic directions connect through bcid = 0; perturbation moves interior
+ * nodes by perturbation*h*sin(2 pi x)sin(2 pi y); rotation (optional, nEl
+ * entries) relabels an element's corners by quarter turns. */
+int selfgpu_mesh2d_structured(int nx, int ny, double x0, double x1, double y0, double y1, int periodicX,
+                              int periodicY, double perturbation, int bcid, const int* rotation,
+                              double* nodeCoords, int* globalNodeIDs, int* sideInfo);
+
+/* Host check of sideInfo (neighbour ids, sides, flips); SELFGPU_ERR_MESH if malformed. */
+int selfgpu_validate_side_info(const int* sideInfo, int nEl);
+
+/* SEMQuad%GenerateFromMesh on the device (src/SELF_Geometry.f90:393-552):
+ * from device nodeCoords (nGeo = 1) and the model's Lagrange matrices (host
+ * pointers: iMatrix of the mesh-to-model interpolant (0:1,0:N), dMatrix,
+ * bMatrix) fill the device arrays x(2,P,P,1,nEl), dxds/dsdx (2,2,P,P,1,nEl),
+ * J(P,P,1,nEl), dsdxBoundary (2,2,P,1,4,nEl), JBoundary(P,1,4,nEl),
+ * nHat(2,P,1,4,nEl), nScale(P,1,4,nEl).  Any output pointer may be NULL
+ * except those the later ones depend on internally (handled with scratch). */
+int selfgpu_semquad_generate(int N, int nEl, const double* nodeCoords_d, const double* meshToModel_iMatrix,
+                             const double* dMatrix, const double* bMatrix, double* x_d, double* dxds_d,
+                             double* dsdx_d, double* J_d, double* dsdxBoundary_d, double* JBoundary_d,
+                             double* nHat_d, double* nScale_d, void* stream);
+
+/* ========================================================= 3. fused engine */
+
+typedef struct selfgpu_model2d selfgpu_model2d;
+
+/* Create an engine for `model` (SELFGPU_MODEL_*), degree N (1..SELFGPU_MAX_N),
+ * nEl elements, arithmetic form SELFGPU_FP64 or SELFGPU_FP32_BULK, on `stream`
+ * (a cudaStream_t, NULL = legacy default stream).  Mirrors Model2D%Init
+ * (src/SELF_Model2D.f90:142-178) minus the buffers the caller already owns. */
+int selfgpu_model2d_create(selfgpu_model2d** out, int model, int N, int nEl, int form, void* stream);
+int selfgpu_model2d_destroy(selfgpu_model2d* m);
+
+/* Operator matrices from Lagrange%Init (host pointers, copied into the handle):
+ * dgMatrix(0:N,0:N), bMatrix(0:N,0:1), qWeights(0:N). */
+int selfgpu_model2d_set_interp(selfgpu_model2d* m, const double* dgMatrix, const double* bMatrix,
+                               const double* qWeights);
+
+/* Geometry (device pointers, caller owned): dsdx interior (2,2,P,P,1,nEl),
+ * J interior (P,P,1,nEl), nHat boundary (2,P,1,4,nEl), nScale boundary
+ * (P,1,4,nEl), sideInfo (5,4,nEl) on the device and a host copy of it, which
+ * is validated here (SELFGPU_ERR_MESH on a malformed record). */
+int selfgpu_model2d_set_geometry(selfgpu_model2d* m, const double* dsdx, const double* J, const double* nHat,
+                                 const double* nScale, const int* sideInfo_d, const int* sideInfo_h);
+
+/* Model state (device, caller owned): solution interior (P,P,nVar,nEl) and
+ * the RK register workSol of the same shape (zero it before the first step;
+ * the reference never uploads it, hazard H21). */
+int selfgpu_model2d_set_state(selfgpu_model2d* m, double* solution, double* workSol);
+
+/* Model-specific device fields (caller owned), by name:
+ *  LSW: "H" interior (P,P,1,nEl), "H.boundary" (P,1,4,nEl), "fCori" interior
+ *  SW : "topography.boundary" (P,1,4,nEl), "gradTopography" (2,P,P,1,nEl)
+ *  CIG: "environmentalsGradient" (2,P,P,2,nEl), "environmentals" (P,P,2,nEl),
+ *       "prescribedSolution.boundary", "prescribedPrimitive.boundary",
+ *       "prescribedDiagnostics.boundary" (P,4,4,nEl each)
+ * A field never set reads as zero. */
+int selfgpu_model2d_set_field(selfgpu_model2d* m, const char* name, const double* ptr);
+
+/* Scalar parameters: g and fCori (LSW/SW), expansion factor Cp/Cv and R (CIG). */
+int selfgpu_model2d_set_params(selfgpu_model2d* m, double g, double fCori, double expansionFactor, double R);
+
+/* Declare that the solution was written outside the engine (SetSolution and
+ * the like): the next tendency or step rebuilds the face-trace cache from it. */
+int selfgpu_model2d_invalidate(selfgpu_model2d* m);
+
+/* One CalculateTendency_Model2D (src/SELF_Model2D.f90:816-859): dSdt (device,
+ * (P,P,nVar,nEl)) = source - weak-form flux divergence, solution unchanged. */
+int selfgpu_model2d_tendency(selfgpu_model2d* m, double* dSdt);
+
+/* nSteps Williamson low-storage RK3 steps of size dt
+ * (LowStorageRK3_timeIntegrator, src/SELF_Model.f90:704-732, stepped by
+ * count): per stage one fused kernel does tendency + UpdateGRK3.  Steps are
+ * replayed from a captured CUDA graph after the first call. */
+int selfgpu_model2d_rk3(selfgpu_model2d* m, double dt, int nSteps);
+
+/* Wait for the engine's stream; returns the first pending CUDA error. */
+int selfgpu_model2d_sync(selfgpu_model2d* m);
+
+/* Scan the solution for NaN/Inf on the device (SELFGPU_ERR_NONFINITE if any). */
+int selfgpu_model2d_check_finite(selfgpu_model2d* m);
+
+/* Number of kernel launches the engine has issued (for accounting). */
+long long selfgpu_model2d_launch_count(const selfgpu_model2d* m);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SELFGPU_H */

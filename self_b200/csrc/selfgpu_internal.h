@@ -1,0 +1,25 @@
+// Internal declarations shared by the libselfgpu translation units.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "../../include/selfgpu.h"
+
+namespace selfgpu {
+
+// Records the calling thread's last error (read back by selfgpu_last_error).
+int set_error(int code, const std::string& msg);
+const char* last_error();
+
+// Host set-up (setup_host.cpp).
+void legendre_quadrature(int N, int type, double* x, double* w);
+int lagrange_init(int N, int ctrlType, int M, int tgtType, double* ctrl, double* tgt, double* bw,
+                  double* qw, double* iM, double* dM, double* dgM, double* bM);
+int mesh2d_structured(int nx, int ny, double x0, double x1, double y0, double y1, int perX, int perY,
+                      double amp, int bcid, const int* rot, double* nodeCoords, int* globalNodeIDs,
+                      int* sideInfo);
+int validate_side_info(const int* sideInfo, int nEl);
+
+}  // namespace selfgpu
