@@ -252,6 +252,7 @@ def run_engine(args, rank, world, local_rank):
         dist.barrier()
     ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     launches = model.LaunchCount() - launches0  # fused-stage launches (plus one trace prologue per solve)
+    persistent = S.lib().selfgpu_model2d_persistent_launch_count(model._h)
     clk = clocks.summary()
     t_max = ms
     if dist:
@@ -312,7 +313,8 @@ def run_engine(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind,
                      "bytes_per_launch": per_launch, "launch_ms": stage_ms,
-                     "kernel": "k_fused_stage<8,PhysCIG,double> (one RK stage over all elements)"},
+                     "kernel": ("k_fused_stage_tma<8,PhysCIG,double>" if persistent else
+                                "k_fused_stage<8,PhysCIG,double>") + " (one RK stage over all elements)"},
         "clocks": clk,
     }
     if not args.no_cpu_baseline:

@@ -289,8 +289,25 @@ int selfgpu_model2d_sync(selfgpu_model2d* m);
 /* Scan the solution for NaN/Inf on the device (SELFGPU_ERR_NONFINITE if any). */
 int selfgpu_model2d_check_finite(selfgpu_model2d* m);
 
-/* Number of kernel launches the engine has issued (for accounting). */
+/* Number of kernel launches the engine has issued (for accounting), and how
+ * many of them ran the persistent bulk-copy kernel. */
 long long selfgpu_model2d_launch_count(const selfgpu_model2d* m);
+long long selfgpu_model2d_persistent_launch_count(const selfgpu_model2d* m);
+
+/* Kernel choice: persistent = 1 (default) uses the warp-specialised kernel
+ * that streams elements through shared memory with bulk asynchronous copies
+ * wherever it applies (even P, 16-byte aligned buffers); 0 forces the
+ * one-CTA-per-element-group kernel. */
+int selfgpu_model2d_set_kernel(selfgpu_model2d* m, int persistent);
+
+/* Failure detection.  Every wait inside the persistent kernel is bounded; a
+ * wait that runs out sets an error word, the kernel stops and returns, and the
+ * next selfgpu_model2d_sync() returns SELFGPU_ERR_TIMEOUT.  set_wait_limit
+ * sets the bound in SM clock cycles (default 4e9, about 2 s).  inject_stall
+ * (for tests of this path) makes the next launches register one element's
+ * copies without issuing them, so its consumers' wait runs out. */
+int selfgpu_model2d_set_wait_limit(selfgpu_model2d* m, long long cycles);
+int selfgpu_model2d_inject_stall(selfgpu_model2d* m, int enable);
 
 #ifdef __cplusplus
 }

@@ -41,6 +41,10 @@ _SIGS = {
     "selfgpu_model2d_sync": (c_int, [c_void_p]),
     "selfgpu_model2d_check_finite": (c_int, [c_void_p]),
     "selfgpu_model2d_launch_count": (c_longlong, [c_void_p]),
+    "selfgpu_model2d_persistent_launch_count": (c_longlong, [c_void_p]),
+    "selfgpu_model2d_set_kernel": (c_int, [c_void_p, c_int]),
+    "selfgpu_model2d_set_wait_limit": (c_int, [c_void_p, c_longlong]),
+    "selfgpu_model2d_inject_stall": (c_int, [c_void_p, c_int]),
     # drop-in wrappers (src/hip/*.cpp, src/models/hip/*.cpp of the reference)
     "ScalarGridInterp_2D_gpu_wrapper": (None, [PP, PP, PP, c_int, c_int, c_int, c_int]),
     "VectorGridInterp_2D_gpu_wrapper": (None, [PP, PP, PP, c_int, c_int, c_int, c_int]),

@@ -12,8 +12,11 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libselfgpu.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
-SOURCES = ["setup_host.cpp", "legacy_ops.cu", "engine.cu"]
-HEADERS = ["selfgpu_internal.h", "physics.cuh", "fused_stage.cuh"]
+# (source, extra flags): the FP64 kernels are built without multiply-add
+# contraction so their roundings follow the reference's CPU path exactly.
+SOURCES = [("setup_host.cpp", []), ("legacy_ops.cu", ["-fmad=false"]), ("stage_fp64.cu", ["-fmad=false"]),
+           ("stage_fp32.cu", []), ("engine.cu", [])]
+HEADERS = ["selfgpu_internal.h", "physics.cuh", "fused_stage.cuh", "fused_stage_tma.cuh", "stage_dispatch.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
               "-Xptxas", "-O3"]
@@ -39,12 +42,12 @@ def build(force=False, verbose=False, ptxas_info=False):
     deps_common = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(inc, "selfgpu.h")]
     objs = []
     jobs = []
-    for src in SOURCES:
+    for src, extra in SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD_DIR, src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + deps_common):
-            cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, "-I", inc, "-c", s, "-o", o]
+            cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-I", inc, "-c", s, "-o", o]
             if ptxas_info and src.endswith(".cu"):
                 cmd += ["-Xptxas", "-v"]
             jobs.append((cmd, src))

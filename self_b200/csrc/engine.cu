@@ -22,46 +22,6 @@ namespace {
 const double kRK3a[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
 const double kRK3g[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
 
-template <int P, class Phys, typename R>
-constexpr int elems_per_block() {
-  int e = 128 / (P * P);
-  if (e < 1) e = 1;
-  while (e > 1 && (size_t)e * sizeof(Smem<P, Phys, R>) > 44 * 1024) --e;
-  return e;
-}
-
-template <int P, class Phys, typename R>
-cudaError_t launch_stage(const StageArgs& a, cudaStream_t st) {
-  constexpr int EPB = elems_per_block<P, Phys, R>();
-  const int grid = (a.nEl + EPB - 1) / EPB;
-  k_fused_stage<P, Phys, R, EPB><<<grid, EPB * P * P, 0, st>>>(a);
-  return cudaGetLastError();
-}
-
-template <class Phys, typename R>
-cudaError_t dispatch_P(int P, const StageArgs& a, cudaStream_t st) {
-  switch (P) {
-    case 2: return launch_stage<2, Phys, R>(a, st);
-    case 3: return launch_stage<3, Phys, R>(a, st);
-    case 4: return launch_stage<4, Phys, R>(a, st);
-    case 5: return launch_stage<5, Phys, R>(a, st);
-    case 6: return launch_stage<6, Phys, R>(a, st);
-    case 7: return launch_stage<7, Phys, R>(a, st);
-    case 8: return launch_stage<8, Phys, R>(a, st);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
-template <typename R>
-cudaError_t dispatch_model(int model, int P, const StageArgs& a, cudaStream_t st) {
-  switch (model) {
-    case SELFGPU_MODEL_LSW: return dispatch_P<PhysLSW, R>(P, a, st);
-    case SELFGPU_MODEL_SW: return dispatch_P<PhysSW, R>(P, a, st);
-    case SELFGPU_MODEL_CIG: return dispatch_P<PhysCIG, R>(P, a, st);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
 __global__ void k_nonfinite(const double* __restrict__ q, long long n, int* flag) {
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
     if (!isfinite(q[k])) {
@@ -87,17 +47,24 @@ struct selfgpu_model2d {
   int vcur = 0;    // index of the velocity buffer the next stage reads (SW)
   bool valid = false;
   int* dflag = nullptr;
+  int* derr = nullptr;  // error word of the persistent kernel's bounded waits
   long long launches = 0;
+  long long tmaLaunches = 0;
+  StageLaunch cfg{true, 0, 148};
   // graph cache: one captured RK step per starting buffer parity
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  long long graphTma[2][2] = {{0, 0}, {0, 0}};
   double graphDt = NAN;
 
   size_t elemBytes() const { return form == SELFGPU_FP64 ? sizeof(double) : sizeof(float); }
 
   cudaError_t launch(StageArgs a) {
     ++launches;
-    return form == SELFGPU_FP64 ? dispatch_model<double>(model, P, a, stream)
-                                : dispatch_model<float>(model, P, a, stream);
+    int tma = 0;
+    cudaError_t e = form == SELFGPU_FP64 ? launch_stage_fp64(model, P, a, cfg, stream, &tma)
+                                         : launch_stage_fp32(model, P, a, cfg, stream, &tma);
+    tmaLaunches += tma;
+    return e;
   }
 
   void drop_graphs() {
@@ -189,11 +156,17 @@ int selfgpu_model2d_create(selfgpu_model2d** out, int model, int N, int nEl, int
       return fail_cuda("selfgpu_model2d_create: trace cache", e);
     }
   }
-  e = cudaMalloc(&m->dflag, sizeof(int));
+  e = cudaMalloc(&m->dflag, 2 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(m->dflag, 0, 2 * sizeof(int));
   if (e != cudaSuccess) {
     selfgpu_model2d_destroy(m);
     return fail_cuda("selfgpu_model2d_create", e);
   }
+  m->derr = m->dflag + 1;
+  cudaDeviceGetAttribute(&m->cfg.smemOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaDeviceGetAttribute(&m->cfg.numSMs, cudaDevAttrMultiProcessorCount, dev);
+  m->base.err = m->derr;
+  m->base.waitCycles = 4000000000LL;  // about 2 s at the B200 boost clock
   m->base.nEl = nEl;
   m->base.g = 1.0;
   m->base.gamma = 1.4;
@@ -304,6 +277,12 @@ static int check_ready(selfgpu_model2d* m, const char* where) {
     return set_error(SELFGPU_ERR_STATE, std::string(where) + ": interp, geometry and state must be set first");
   if (m->model == SELFGPU_MODEL_LSW && (!m->base.fld[0] || !m->base.fld[1]))
     return set_error(SELFGPU_ERR_STATE, std::string(where) + ": LinearShallowWater needs H and H.boundary");
+  if (m->model == SELFGPU_MODEL_CIG) {
+    const int np = (m->base.fld[2] != nullptr) + (m->base.fld[3] != nullptr) + (m->base.fld[4] != nullptr);
+    if (np != 0 && np != 3)
+      return set_error(SELFGPU_ERR_STATE, std::string(where) +
+                                              ": set all three prescribed boundary fields or none of them");
+  }
   return SELFGPU_OK;
 }
 
@@ -348,9 +327,11 @@ int selfgpu_model2d_rk3(selfgpu_model2d* m, double dt, int nSteps) {
         cudaGraph_t graph = nullptr;
         e = cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-          const long long l0 = m->launches;
+          const long long l0 = m->launches, t0 = m->tmaLaunches;
           e = m->step(dt);
+          m->graphTma[c0][v0] = m->tmaLaunches - t0;
           m->launches = l0;
+          m->tmaLaunches = t0;
           cudaError_t e2 = cudaStreamEndCapture(m->stream, &graph);
           if (e == cudaSuccess) e = e2;
         }
@@ -374,6 +355,7 @@ int selfgpu_model2d_rk3(selfgpu_model2d* m, double dt, int nSteps) {
     e = cudaGraphLaunch(g, m->stream);
     if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_rk3: graph launch", e);
     m->launches += 3;
+    m->tmaLaunches += m->graphTma[m->cur][m->vcur];
     m->cur = 1 - m->cur;  // three swaps per step
     if (m->model == SELFGPU_MODEL_SW) m->vcur = 1 - m->vcur;
   }
@@ -385,8 +367,40 @@ int selfgpu_model2d_sync(selfgpu_model2d* m) {
   cudaError_t e = cudaStreamSynchronize(m->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_sync", e);
+  int werr = 0;
+  e = cudaMemcpy(&werr, m->derr, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_sync", e);
+  if (werr) {
+    cudaMemset(m->derr, 0, sizeof(int));
+    m->valid = false;
+    return set_error(SELFGPU_ERR_TIMEOUT,
+                     "selfgpu_model2d_sync: a bounded device wait ran out; the solution of this call is invalid");
+  }
   return SELFGPU_OK;
 }
+
+int selfgpu_model2d_set_wait_limit(selfgpu_model2d* m, long long cycles) {
+  if (!m || cycles < 1000) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_wait_limit: bad arguments");
+  m->base.waitCycles = cycles;
+  m->drop_graphs();
+  return SELFGPU_OK;
+}
+
+int selfgpu_model2d_inject_stall(selfgpu_model2d* m, int enable) {
+  if (!m) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_inject_stall: null handle");
+  m->base.debugStarve = enable ? 1 : 0;
+  m->drop_graphs();
+  return SELFGPU_OK;
+}
+
+int selfgpu_model2d_set_kernel(selfgpu_model2d* m, int persistent) {
+  if (!m) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_kernel: null handle");
+  m->cfg.allowTma = persistent != 0;
+  m->drop_graphs();
+  return SELFGPU_OK;
+}
+
+long long selfgpu_model2d_persistent_launch_count(const selfgpu_model2d* m) { return m ? m->tmaLaunches : 0; }
 
 int selfgpu_model2d_check_finite(selfgpu_model2d* m) {
   if (!m || !m->haveState) return set_error(SELFGPU_ERR_STATE, "selfgpu_model2d_check_finite: no state bound");

@@ -1,0 +1,482 @@
+// Persistent, warp-specialised variant of the fused stage kernel.
+//
+// One CTA per SM.  Warp 0 is the producer: for every element the CTA owns it
+// issues 1-D bulk asynchronous copies (cp.async.bulk, the non-tensor TMA path)
+// of the element's contiguous blocks -- solution, RK register, dsdx, J, nHat,
+// nScale, sideInfo, model fields -- and of the four neighbour trace blocks
+// named by sideInfo, into a shared-memory buffer whose mbarrier counts the
+// bytes in.  The remaining warps form C consumer groups of TPE threads (one
+// thread per node); each group owns two buffers, so the copies for its next
+// element are in flight while it computes the current one.  No thread waits
+// on global-memory latency except the producer's batched sideInfo reads.
+//
+// Every wait is bounded (StageArgs::waitCycles): on timeout the kernel records
+// an error word, stops issuing copies, waits (again bounded) for copies it has
+// already issued and returns; the host reports SELFGPU_ERR_TIMEOUT.
+//
+// Requires an even P (all per-element block sizes are then multiples of 16
+// bytes) and 16-byte aligned base pointers; the engine falls back to
+// k_fused_stage otherwise.
+#pragma once
+
+#include "fused_stage.cuh"
+
+namespace selfgpu {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: true when the phase with this parity has completed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long cycles) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (true) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (clock64() - t0 > cycles) return false;
+    __nanosleep(64);
+  }
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void named_bar(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// Runtime layout of one element buffer (byte offsets; -1 = piece absent) and
+// of the CTA's shared memory.  Built on the host by make_tma_plan().
+struct TmaPlan {
+  int groups;      // consumer groups per CTA
+  int slotBytes;   // bytes of one element buffer
+  int oQ, oG, oDsdx, oJ, oNhat, oNs, oSi, oNbr;
+  int oX[5];       // model fields: LSW (H, Hb, fC), SW (topoB, grad), CIG (envG, drag, presc x3 -> oX[2..4])
+  int oVelOwn, oVelNbr;
+  int oMats, oFlags, oSlots, oGroups, groupBytes, smemBytes;
+};
+
+template <int P, class Phys, typename R>
+struct TmaTraits {
+  static constexpr int PP = P * P, NV = Phys::NV, NT = Phys::NT, NF = Phys::NF;
+  static constexpr int TS = trace_side_stride<P, NT, R>();
+  static constexpr int TPE = (PP + 31) / 32 * 32;
+  static constexpr int kMaxGroups = 8;
+  static constexpr int kThreadsMax = 32 + kMaxGroups * TPE;
+  // per-group compute arrays (bulk type)
+  static constexpr int groupBytes = (int)(((NF * PP + 2 * NV * PP + 4 * NV * P) * sizeof(R) + 127) / 128 * 128);
+};
+
+template <int P, class Phys, typename R>
+__global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
+    k_fused_stage_tma(const StageArgs a, const TmaPlan pl) {
+  using T = TmaTraits<P, Phys, R>;
+  constexpr int NV = T::NV, NT = T::NT, NF = T::NF, PP = T::PP, TS = T::TS, TPE = T::TPE, N = P - 1;
+  constexpr bool kLSW = (NV == 3 && !Phys::kLaggedVelocity);
+  constexpr bool kSW = Phys::kLaggedVelocity;
+  constexpr bool kCIG = (NV == 4);
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int C = pl.groups;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* empty = full + 2 * C;
+  double* sdg = reinterpret_cast<double*>(smem + pl.oMats);
+  double* sb = sdg + PP;
+  double* srw = sb + 2 * P;
+  volatile int* gflag = reinterpret_cast<volatile int*>(smem + pl.oFlags);
+  unsigned char* slots = smem + pl.oSlots;
+
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 2 * C; ++k) {
+      mbar_init(&full[k], 1);
+      mbar_init(&empty[k], 1);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int k = threadIdx.x; k < PP; k += blockDim.x) sdg[k] = a.dgM[k];
+  for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) sb[k] = a.bM[k];
+  for (int k = threadIdx.x; k < P; k += blockDim.x) srw[k] = a.qw[k];
+  __syncthreads();
+
+  const long long nMine =
+      (long long)blockIdx.x < a.nEl ? ((long long)a.nEl - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  const int warp = threadIdx.x >> 5;
+  const bool rk = (a.mode == MODE_RK);
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    const int lane = threadIdx.x & 31;
+    bool abort = false;
+    long long issued = 0;
+    for (long long k0 = 0; k0 < nMine && !abort; k0 += 32) {
+      // each lane fetches the connectivity of one element of this batch
+      int nbE[4] = {0, 0, 0, 0}, nbS[4] = {0, 0, 0, 0};  // e2 (1-based, 0 = none), s2 (0-based)
+      if (k0 + lane < nMine) {
+        const long long e = blockIdx.x + (k0 + lane) * gridDim.x;
+        const int* si = a.sideInfo + 20 * e;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          if (si[5 * s + 4] == 0) {
+            nbE[s] = si[5 * s + 2];
+            nbS[s] = si[5 * s + 3] / 10 - 1;
+          }
+        }
+      }
+      const int nb = (int)min(32LL, nMine - k0);
+      for (int b = 0; b < nb; ++b) {
+        int e2[4], s2[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          e2[s] = __shfl_sync(0xffffffffu, nbE[s], b);
+          s2[s] = __shfl_sync(0xffffffffu, nbS[s], b);
+        }
+        const long long k = k0 + b;
+        const int g = (int)(k % C);
+        const long long jj = k / C;
+        const int buf = (int)(jj & 1);
+        const uint32_t par = (uint32_t)((jj >> 1) & 1);
+        if (lane == 0) {
+          if (!mbar_wait(&empty[2 * g + buf], par ^ 1u, a.waitCycles)) {
+            abort = true;
+          } else {
+            const long long e = blockIdx.x + k * gridDim.x;
+            unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
+            uint64_t* bar = &full[2 * g + buf];
+            const uint32_t qb = NV * PP * 8;
+            uint32_t bytes = qb + 4 * PP * 8 + PP * 8 + 8 * P * 8 + 4 * P * 8 + 80;
+            if (rk) bytes += qb;
+            const uint32_t tsb = TS * sizeof(R);
+            const uint32_t vnb = 2 * P * sizeof(R);
+            int nInt = 0;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) nInt += (e2[s] != 0);
+            bytes += nInt * tsb;
+            if constexpr (kSW) bytes += 8 * P * sizeof(R) + nInt * vnb;
+            // model fields
+            uint32_t xb[5] = {0, 0, 0, 0, 0};
+            if constexpr (kLSW) {
+              xb[0] = PP * 8;
+              xb[1] = 4 * P * 8;
+              xb[2] = a.fld[2] ? PP * 8 : 0;
+            } else if constexpr (kSW) {
+              xb[0] = a.fld[0] ? 4 * P * 8 : 0;
+              xb[1] = a.fld[1] ? 2 * PP * 8 : 0;
+            } else {
+              xb[0] = a.fld[0] ? 2 * PP * 8 : 0;
+              xb[1] = a.fld[1] ? PP * 8 : 0;
+              xb[2] = xb[3] = xb[4] = a.fld[2] ? 16 * P * 8 : 0;
+            }
+            for (int x = 0; x < 5; ++x) bytes += xb[x];
+            mbar_arrive_expect_tx(bar, bytes);
+            if (!(a.debugStarve && blockIdx.x == 0 && k == 0)) {
+              bulk_g2s(sl + pl.oQ, a.q + (size_t)e * NV * PP, qb, bar);
+              if (rk) bulk_g2s(sl + pl.oG, a.G + (size_t)e * NV * PP, qb, bar);
+              bulk_g2s(sl + pl.oDsdx, a.dsdx + (size_t)e * 4 * PP, 4 * PP * 8, bar);
+              bulk_g2s(sl + pl.oJ, a.J + (size_t)e * PP, PP * 8, bar);
+              bulk_g2s(sl + pl.oNhat, a.nHat + (size_t)e * 8 * P, 8 * P * 8, bar);
+              bulk_g2s(sl + pl.oNs, a.nScale + (size_t)e * 4 * P, 4 * P * 8, bar);
+              bulk_g2s(sl + pl.oSi, a.sideInfo + (size_t)e * 20, 80, bar);
+              const R* trIn = reinterpret_cast<const R*>(a.trIn);
+#pragma unroll
+              for (int s = 0; s < 4; ++s)
+                if (e2[s] != 0)
+                  bulk_g2s(sl + pl.oNbr + s * tsb, trIn + (size_t)TS * (s2[s] + 4 * (size_t)(e2[s] - 1)), tsb, bar);
+              if constexpr (kSW) {
+                const R* vIn = reinterpret_cast<const R*>(a.velIn);
+                bulk_g2s(sl + pl.oVelOwn, vIn + (size_t)e * 8 * P, 8 * P * sizeof(R), bar);
+#pragma unroll
+                for (int s = 0; s < 4; ++s)
+                  if (e2[s] != 0)
+                    bulk_g2s(sl + pl.oVelNbr + s * vnb, vIn + (size_t)2 * P * (s2[s] + 4 * (size_t)(e2[s] - 1)), vnb,
+                             bar);
+              }
+              if constexpr (kLSW) {
+                bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * PP, xb[0], bar);
+                bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 4 * P, xb[1], bar);
+                if (xb[2]) bulk_g2s(sl + pl.oX[2], a.fld[2] + (size_t)e * PP, xb[2], bar);
+              } else if constexpr (kSW) {
+                if (xb[0]) bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * 4 * P, xb[0], bar);
+                if (xb[1]) bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 2 * PP, xb[1], bar);
+              } else {
+                if (xb[0]) bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * 4 * PP, xb[0], bar);
+                if (xb[1]) bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 2 * PP + PP, xb[1], bar);
+                if (xb[2])
+                  for (int x = 2; x < 5; ++x) bulk_g2s(sl + pl.oX[x], a.fld[x] + (size_t)e * 16 * P, xb[x], bar);
+              }
+            }
+            issued = k + 1;
+          }
+        }
+        abort = __shfl_sync(0xffffffffu, abort ? 1 : 0, 0) != 0;
+        if (abort) break;
+      }
+    }
+    if (lane == 0 && abort) {
+      if (a.err) atomicExch(a.err, 1);
+      // Wait (bounded) for the copies already issued into buffers no consumer
+      // will read any more, so none is in flight when the CTA exits.
+      for (long long k = (issued > 2 * C ? issued - 2 * C : 0); k < issued; ++k) {
+        const int g = (int)(k % C);
+        const long long jj = k / C;
+        mbar_wait(&full[2 * g + (int)(jj & 1)], (uint32_t)((jj >> 1) & 1), a.waitCycles);
+      }
+    }
+    return;
+  }
+
+  // -------------------------------------------------------------- consumers
+  const int g = (threadIdx.x - 32) / TPE;
+  const int t = (threadIdx.x - 32) % TPE;
+  if (g >= C) return;
+  const int barId = 1 + g;
+  const bool active = t < PP;
+  const int i = t % P, j = t / P;
+  R* gfld = reinterpret_cast<R*>(smem + pl.oGroups + (size_t)g * pl.groupBytes);  // [NF][PP]
+  R* gFc = gfld + NF * PP;                                                          // [2][NV][PP]
+  R* gfb = gFc + 2 * NV * PP;                                                       // [4][NV][P]
+  R* trOut = reinterpret_cast<R*>(a.trOut);
+
+  for (long long jj = 0;; ++jj) {
+    const long long k = g + jj * C;
+    if (k >= nMine) break;
+    const long long e = blockIdx.x + k * gridDim.x;
+    const int buf = (int)(jj & 1);
+    const uint32_t par = (uint32_t)((jj >> 1) & 1);
+    const unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
+    if (t == 0) gflag[g] = mbar_wait(&full[2 * g + buf], par, a.waitCycles) ? 1 : 0;
+    named_bar(barId, TPE);
+    if (!gflag[g]) {
+      if (t == 0 && a.err) atomicExch(a.err, 1);
+      break;
+    }
+    const double* sq = reinterpret_cast<const double*>(sl + pl.oQ);
+    const int* ssi = reinterpret_cast<const int*>(sl + pl.oSi);
+
+    // ---- A: solution, auxiliaries, contravariant flux
+    R f[NF];
+    double na[3] = {0.0, 0.0, 0.0};
+    if (active) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) f[v] = (R)sq[t + PP * v];
+      Phys::template node<R>(f, a);
+#pragma unroll
+      for (int v = 0; v < NF; ++v) gfld[v * PP + t] = f[v];
+      if constexpr (kLSW) {
+        na[0] = reinterpret_cast<const double*>(sl + pl.oX[0])[t];
+        if (pl.oX[2] >= 0 && a.fld[2]) na[1] = reinterpret_cast<const double*>(sl + pl.oX[2])[t];
+      } else if constexpr (kSW) {
+        if (a.fld[1]) {
+          const double* gg = reinterpret_cast<const double*>(sl + pl.oX[1]);
+          na[0] = gg[2 * t];
+          na[1] = gg[2 * t + 1];
+        }
+      } else {
+        if (a.fld[0]) {
+          const double* gg = reinterpret_cast<const double*>(sl + pl.oX[0]);
+          na[0] = gg[2 * t];
+          na[1] = gg[2 * t + 1];
+        }
+        if (a.fld[1]) na[2] = reinterpret_cast<const double*>(sl + pl.oX[1])[t];
+      }
+      R Fx[NV], Fy[NV];
+      Phys::template flux<R>(f, na, a, Fx, Fy);
+      const double2* gp = reinterpret_cast<const double2*>(sl + pl.oDsdx) + 2 * t;
+      const double2 c1 = gp[0], c2 = gp[1];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        gFc[v * PP + t] = (R)c1.x * Fx[v] + (R)c1.y * Fy[v];
+        gFc[(NV + v) * PP + t] = (R)c2.x * Fx[v] + (R)c2.y * Fy[v];
+      }
+    }
+    named_bar(barId, TPE);
+
+    // ---- C: faces (own traces interpolated here, exterior from the buffer)
+    if (t < 4 * P) {
+      const int s1 = t / P, ii = t % P;
+      const int bcid = ssi[5 * s1 + 4];
+      const bool physical = (bcid != 0) && (ssi[5 * s1 + 2] == 0);
+      const int flip = ssi[5 * s1 + 3] % 10;
+      const R* nbr = reinterpret_cast<const R*>(sl + pl.oNbr + s1 * TS * sizeof(R));
+      const int i2 = flip ? N - ii : ii;
+      R L[NT], X[NT];
+#pragma unroll
+      for (int kf = 0; kf < NT; ++kf) {
+        L[kf] = face_trace<P, R>(gfld + kf * PP, sb, s1, ii);
+        X[kf] = (bcid == 0) ? nbr[i2 + P * kf] : (R)0;
+      }
+      const double2 nh = reinterpret_cast<const double2*>(sl + pl.oNhat)[ii + P * s1];
+      const double ns = reinterpret_cast<const double*>(sl + pl.oNs)[ii + P * s1];
+      double fx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      if constexpr (kLSW) {
+        fx[0] = reinterpret_cast<const double*>(sl + pl.oX[1])[ii + P * s1];
+      } else if constexpr (kSW) {
+        if (physical && a.fld[0]) fx[0] = reinterpret_cast<const double*>(sl + pl.oX[0])[ii + P * s1];
+      } else {
+        if (physical && a.fld[2]) {
+          const double* ps = reinterpret_cast<const double*>(sl + pl.oX[2]);
+          const double* pp = reinterpret_cast<const double*>(sl + pl.oX[3]);
+          const double* pd = reinterpret_cast<const double*>(sl + pl.oX[4]);
+          const int b = ii + P * 4 * s1;
+          for (int v = 0; v < 4; ++v) fx[v] = ps[b + v * P];
+          fx[4] = pp[b];
+          fx[5] = pp[b + P];
+          fx[6] = pp[b + 3 * P];
+          fx[7] = pd[b + P];
+          fx[8] = pd[b + 2 * P];
+        }
+      }
+      R velL[2] = {(R)0, (R)0}, velR[2] = {(R)0, (R)0};
+      if constexpr (kSW) {
+        const R* vo = reinterpret_cast<const R*>(sl + pl.oVelOwn);
+        velL[0] = vo[ii + P * (0 + 2 * s1)];
+        velL[1] = vo[ii + P * (1 + 2 * s1)];
+        if (bcid == 0) {
+          const R* vn = reinterpret_cast<const R*>(sl + pl.oVelNbr + s1 * 2 * P * sizeof(R));
+          velR[0] = vn[i2];
+          velR[1] = vn[i2 + P];
+        }
+        R* vOut = reinterpret_cast<R*>(a.velOut);
+        vOut[ii + P * (0 + 2 * (s1 + 4 * e))] = L[0] / L[2];
+        vOut[ii + P * (1 + 2 * (s1 + 4 * e))] = L[1] / L[2];
+      }
+      R out[NV];
+      Phys::template face<R>(bcid, physical, L, X, velL, velR, nh.x, nh.y, ns, fx, a, out);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) gfb[(s1 * NV + v) * P + ii] = out[v];
+    }
+    named_bar(barId, TPE);
+
+    // ---- D: weak divergence + lift, 1/J, source, RK update
+    if (active) {
+      R Src[NV];
+      Phys::template source<R>(f, na, a, Src);
+      const double Jij = reinterpret_cast<const double*>(sl + pl.oJ)[t];
+      const double* sG = reinterpret_cast<const double*>(sl + pl.oG);
+      const R wi = (R)srw[i], wj = (R)srw[j];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const R* F1 = gFc + v * PP;
+        const R* F2 = gFc + (NV + v) * PP;
+        R d = (R)0;
+#pragma unroll
+        for (int m = 0; m < P; ++m) d = d + (R)sdg[m + P * i] * F1[m + P * j] + (R)sdg[m + P * j] * F2[i + P * m];
+        d = d + ((R)sb[i + P] * gfb[(1 * NV + v) * P + j] + (R)sb[i] * gfb[(3 * NV + v) * P + j]) / wi +
+            ((R)sb[j + P] * gfb[(2 * NV + v) * P + i] + (R)sb[j] * gfb[(0 * NV + v) * P + i]) / wj;
+        const double dsdt = (double)Src[v] - (double)d / Jij;
+        const size_t gi = t + (size_t)PP * (v + NV * (size_t)e);
+        if (rk) {
+          const double Gn = a.rk_a * sG[t + PP * v] + dsdt;
+          a.G[gi] = Gn;
+          const double qn = sq[t + PP * v] + a.rk_gdt * Gn;
+          a.q[gi] = qn;
+          f[v] = (R)qn;
+        } else {
+          a.dSdt[gi] = dsdt;
+        }
+      }
+      if (rk) {
+        Phys::template node<R>(f, a);
+#pragma unroll
+        for (int v = 0; v < NF; ++v) gfld[v * PP + t] = f[v];
+      }
+    }
+    named_bar(barId, TPE);  // every read of this buffer is done
+    if (t == 0) mbar_arrive(&empty[2 * g + buf]);
+
+    // ---- E: traces of the updated solution -> trace cache
+    if (rk) {
+      R* o = trOut + (size_t)4 * TS * e;
+      for (int kk = t; kk < 4 * NT * P; kk += TPE) {
+        const int ii = kk % P, fs = kk / P, fi = fs % NT, s1 = fs / NT;
+        o[ii + P * fi + TS * s1] = face_trace<P, R>(gfld + fi * PP, sb, s1, ii);
+      }
+    }
+    named_bar(barId, TPE);
+  }
+}
+
+// Host-side plan for k_fused_stage_tma given the smem budget.
+template <int P, class Phys, typename R>
+inline bool make_tma_plan(const StageArgs& a, int smemLimit, TmaPlan& pl) {
+  using T = TmaTraits<P, Phys, R>;
+  constexpr int PP = T::PP, NV = T::NV, TS = T::TS;
+  constexpr bool kLSW = (NV == 3 && !Phys::kLaggedVelocity);
+  constexpr bool kSW = Phys::kLaggedVelocity;
+  if (P % 2 != 0) return false;
+  int o = 0;
+  auto put = [&](int bytes) {
+    int at = o;
+    o += (bytes + 15) / 16 * 16;
+    return at;
+  };
+  pl.oQ = put(NV * PP * 8);
+  pl.oG = put(NV * PP * 8);
+  pl.oDsdx = put(4 * PP * 8);
+  pl.oJ = put(PP * 8);
+  pl.oNhat = put(8 * P * 8);
+  pl.oNs = put(4 * P * 8);
+  pl.oSi = put(80);
+  pl.oNbr = put(4 * TS * (int)sizeof(R));
+  for (int x = 0; x < 5; ++x) pl.oX[x] = -1;
+  pl.oVelOwn = pl.oVelNbr = -1;
+  if (kLSW) {
+    pl.oX[0] = put(PP * 8);
+    pl.oX[1] = put(4 * P * 8);
+    if (a.fld[2]) pl.oX[2] = put(PP * 8);
+  } else if (kSW) {
+    if (a.fld[0]) pl.oX[0] = put(4 * P * 8);
+    if (a.fld[1]) pl.oX[1] = put(2 * PP * 8);
+    pl.oVelOwn = put(8 * P * (int)sizeof(R));
+    pl.oVelNbr = put(8 * P * (int)sizeof(R));
+  } else {
+    if (a.fld[0]) pl.oX[0] = put(2 * PP * 8);
+    if (a.fld[1]) pl.oX[1] = put(PP * 8);
+    if (a.fld[2])
+      for (int x = 2; x < 5; ++x) pl.oX[x] = put(16 * P * 8);
+  }
+  pl.slotBytes = (o + 127) / 128 * 128;
+  pl.groupBytes = T::groupBytes;
+  for (int C = T::kMaxGroups; C >= 1; --C) {
+    int s = 0;
+    s += 4 * C * 8;  // barriers
+    s = (s + 15) / 16 * 16;
+    const int oMats = s;
+    s += (PP + 3 * P) * 8;
+    const int oFlags = s;
+    s += C * 4;
+    s = (s + 127) / 128 * 128;
+    const int oSlots = s;
+    s += 2 * C * pl.slotBytes;
+    const int oGroups = s;
+    s += C * pl.groupBytes;
+    if (s <= smemLimit) {
+      pl.groups = C;
+      pl.oMats = oMats;
+      pl.oFlags = oFlags;
+      pl.oSlots = oSlots;
+      pl.oGroups = oGroups;
+      pl.smemBytes = s;
+      return true;
+    }
+  }
+  return false;
+}
+
+}  // namespace selfgpu

@@ -358,6 +358,8 @@ __global__ void k_side_exchange(double* __restrict__ ext, const double* __restri
     if (elemToRank != nullptr && elemToRank[e2g - 1] != rankId) continue;
     const int s2 = si[3] / 10, flip = si[3] - s2 * 10;
     const long long e2 = (long long)e2g - 1 - offset;
+    const long long nEl = n / (4LL * C * P * nVar);
+    if (e2 < 0 || e2 >= nEl || s2 < 1 || s2 > 4) continue;  // malformed record: leave ext untouched
     int i2;
     if (flip == 0) i2 = i1;
     else if (flip == 1) i2 = N - i1;

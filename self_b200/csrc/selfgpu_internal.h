@@ -22,4 +22,20 @@ int mesh2d_structured(int nx, int ny, double x0, double x1, double y0, double y1
                       int* sideInfo);
 int validate_side_info(const int* sideInfo, int nEl);
 
+// Fused stage launches (stage_fp64.cu / stage_fp32.cu).
+struct StageArgs;
+struct StageLaunch {
+  bool allowTma;   // use the persistent bulk-copy kernel where it applies
+  int smemOptin;   // opt-in shared memory per block (bytes)
+  int numSMs;
+};
+}  // namespace selfgpu
+
+#include <cuda_runtime.h>
+
+namespace selfgpu {
+cudaError_t launch_stage_fp64(int model, int P, const StageArgs& a, const StageLaunch& L, cudaStream_t st,
+                              int* usedTma);
+cudaError_t launch_stage_fp32(int model, int P, const StageArgs& a, const StageLaunch& L, cudaStream_t st,
+                              int* usedTma);
 }  // namespace selfgpu

@@ -1,0 +1,81 @@
+// Host-side launch of the fused stage kernels for one bulk type R.  Included
+// by stage_fp64.cu (built with -fmad=false so that every FP64 operation rounds
+// exactly as the reference's CPU path does) and stage_fp32.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "fused_stage.cuh"
+#include "fused_stage_tma.cuh"
+#include "selfgpu_internal.h"
+
+namespace selfgpu {
+
+template <int P, class Phys, typename R>
+constexpr int elems_per_block() {
+  int e = 128 / (P * P);
+  if (e < 1) e = 1;
+  while (e > 1 && (size_t)e * sizeof(Smem<P, Phys, R>) > 44 * 1024) --e;
+  return e;
+}
+
+inline bool aligned16(const void* p) { return ((uintptr_t)p % 16) == 0; }
+
+template <int P, class Phys, typename R>
+cudaError_t launch_one(const StageArgs& a, const StageLaunch& L, cudaStream_t st, int* usedTma) {
+  *usedTma = 0;
+  if constexpr (P % 2 == 0) {
+    bool ok = L.allowTma && a.mode != MODE_TRACES && aligned16(a.q) && aligned16(a.G) && aligned16(a.dsdx) &&
+              aligned16(a.J) && aligned16(a.nHat) && aligned16(a.nScale) && aligned16(a.sideInfo) &&
+              aligned16(a.trIn) && (a.velIn == nullptr || aligned16(a.velIn));
+    for (int k = 0; k < 5; ++k) ok = ok && (a.fld[k] == nullptr || aligned16(a.fld[k]));
+    TmaPlan pl{};
+    if (ok && make_tma_plan<P, Phys, R>(a, L.smemOptin, pl)) {
+      static bool attrSet = false;  // one instantiation per (P, Phys, R)
+      if (!attrSet) {
+        cudaError_t e = cudaFuncSetAttribute(k_fused_stage_tma<P, Phys, R>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, L.smemOptin);
+        if (e != cudaSuccess) return e;
+        attrSet = true;
+      }
+      using T = TmaTraits<P, Phys, R>;
+      const int grid = a.nEl < L.numSMs ? a.nEl : L.numSMs;
+      k_fused_stage_tma<P, Phys, R><<<grid, 32 + pl.groups * T::TPE, pl.smemBytes, st>>>(a, pl);
+      *usedTma = 1;
+      return cudaGetLastError();
+    }
+  }
+  constexpr int EPB = elems_per_block<P, Phys, R>();
+  const int grid = (a.nEl + EPB - 1) / EPB;
+  k_fused_stage<P, Phys, R, EPB><<<grid, EPB * P * P, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <class Phys, typename R>
+cudaError_t launch_P(int P, const StageArgs& a, const StageLaunch& L, cudaStream_t st, int* usedTma) {
+  switch (P) {
+    case 2: return launch_one<2, Phys, R>(a, L, st, usedTma);
+    case 3: return launch_one<3, Phys, R>(a, L, st, usedTma);
+    case 4: return launch_one<4, Phys, R>(a, L, st, usedTma);
+    case 5: return launch_one<5, Phys, R>(a, L, st, usedTma);
+    case 6: return launch_one<6, Phys, R>(a, L, st, usedTma);
+    case 7: return launch_one<7, Phys, R>(a, L, st, usedTma);
+    case 8: return launch_one<8, Phys, R>(a, L, st, usedTma);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <typename R>
+cudaError_t launch_stage_impl(int model, int P, const StageArgs& a, const StageLaunch& L, cudaStream_t st,
+                              int* usedTma) {
+  switch (model) {
+    case SELFGPU_MODEL_LSW: return launch_P<PhysLSW, R>(P, a, L, st, usedTma);
+    case SELFGPU_MODEL_SW: return launch_P<PhysSW, R>(P, a, L, st, usedTma);
+    case SELFGPU_MODEL_CIG: return launch_P<PhysCIG, R>(P, a, L, st, usedTma);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace selfgpu

@@ -1,0 +1,11 @@
+// FP32-bulk instantiation of the fused stage kernels: fluxes, traces and the
+// divergence in float (with multiply-add contraction); metric terms, sources'
+// fields and the RK accumulation of the solution stay in double.
+#include "stage_dispatch.cuh"
+
+namespace selfgpu {
+cudaError_t launch_stage_fp32(int model, int P, const StageArgs& a, const StageLaunch& L, cudaStream_t st,
+                              int* usedTma) {
+  return launch_stage_impl<float>(model, P, a, L, st, usedTma);
+}
+}  // namespace selfgpu

@@ -15,13 +15,26 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-13
 
 
+_KEEP = []  # device buffers handed to asynchronous wrappers stay referenced until the test ends
+
+
 def D(a, dtype=torch.float64):
     import self_b200 as S
-    return S.to_device(a, dtype=dtype)
+    t = S.to_device(a, dtype=dtype)
+    _KEEP.append(t)
+    return t
+
+
+@pytest.fixture(autouse=True)
+def _release_buffers():
+    yield
+    torch.cuda.synchronize()
+    _KEEP.clear()
 
 
 def H(t, shape):
     import self_b200 as S
+    torch.cuda.synchronize()
     return S.to_host(t).reshape(shape, order="F")
 
 
