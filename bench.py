@@ -211,6 +211,7 @@ def run_engine(args, rank, world, local_rank):
     mesh = S.Mesh2D(NX, NX, periodic=(True, True), perturbation=0.02)
     geo = S.SEMQuad(interp, mesh)
     model = S.CompressibleIdealGas2D(mesh, geo, stream=stream.cuda_stream)
+    S.lib().selfgpu_model2d_set_kernel(model._h, 1 if args.kernel == "persistent" else 0)
     q0 = initial_state(geo.x)
     torch.cuda.synchronize()
     # CFL time step: dt = CFL * ArcMin / max(|u| + c)
@@ -329,6 +330,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="selfgpu", choices=["selfgpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel", default="persistent", choices=["persistent", "per-element"],
+                    help="stage kernel: persistent bulk-copy kernel or one CTA per element group")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -93,6 +93,8 @@ struct PhysLSW {
   template <typename R>
   __device__ static void node(R*, const StageArgs&) {}
   template <typename R>
+  __device__ static void node_flux(R*, const StageArgs&) {}
+  template <typename R>
   __device__ static void flux(const R* f, const double* a, const StageArgs& s, R Fx[3], R Fy[3]) {
     const R H = (R)a[0], g = (R)s.g;  // src/models/SELF_LinearShallowWater.f90:470-490
     Fx[0] = g * f[2];
@@ -132,6 +134,10 @@ struct PhysSW {
     const R H = f[2];  // src/models/SELF_ShallowWater.f90:205-216
     f[3] = f[0] / H;
     f[4] = f[1] / H;
+  }
+  template <typename R>
+  __device__ static void node_flux(R* f, const StageArgs& s) {
+    node<R>(f, s);
   }
   template <typename R>
   __device__ static void flux(const R* f, const double*, const StageArgs& s, R Fx[3], R Fy[3]) {
@@ -175,6 +181,17 @@ struct PhysCIG {
     f[6] = p;
     f[7] = h;
     f[8] = c;
+  }
+  // The volume flux needs u, v, p and rhoH only (no sound speed).
+  template <typename R>
+  __device__ static void node_flux(R* f, const StageArgs& s) {
+    const R u = f[0] / f[2], v = f[1] / f[2];
+    const R ke = (R)0.5 * (f[0] * u + f[1] * v);
+    const R p = ((R)s.gamma - (R)1) * (f[3] - ke);
+    f[4] = u;
+    f[5] = v;
+    f[6] = p;
+    f[7] = f[3] + p;
   }
   template <typename R>
   __device__ static void flux(const R* f, const double*, const StageArgs&, R Fx[4], R Fy[4]) {
@@ -256,6 +273,21 @@ __device__ __forceinline__ void face_aux_global(const StageArgs& s, int side, in
 // Boundary interpolation of one traced field at face node ii of side s1
 // (src/SELF_Lagrange.f90:2241-2270): S and N run along j at fixed i, E and W
 // along i at fixed j.
+// Same sums without a branch on the side: S/N step through j (stride P) from
+// node (ii, 0), E/W through i (stride 1) from node (0, ii); S/W use the left
+// boundary row of bMatrix, E/N the right one.
+template <int P, typename R>
+__device__ __forceinline__ R face_trace_uniform(const R* fv, const double* sb, int s1, int ii) {
+  const bool sn = (s1 & 1) == 0;
+  const int base = sn ? ii : P * ii;
+  const int stride = sn ? P : 1;
+  const double* b = sb + ((s1 == 1 || s1 == 2) ? P : 0);
+  R acc = (R)0;
+#pragma unroll
+  for (int m = 0; m < P; ++m) acc = acc + (R)b[m] * fv[base + stride * m];
+  return acc;
+}
+
 template <int P, typename R>
 __device__ __forceinline__ R face_trace(const R* fv, const double* sb, int s1, int ii) {
   R acc = (R)0;

@@ -68,7 +68,7 @@ __device__ __forceinline__ void named_bar(int id, int nthreads) {
 struct TmaPlan {
   int groups;      // consumer groups per CTA
   int slotBytes;   // bytes of one element buffer
-  int oQ, oG, oDsdx, oJ, oNhat, oNs, oSi, oNbr;
+  int oQ, oDsdx, oNhat, oNs, oSi, oOwn, oNbr;
   int oX[5];       // model fields: LSW (H, Hb, fC), SW (topoB, grad), CIG (envG, drag, presc x3 -> oX[2..4])
   int oVelOwn, oVelNbr;
   int oMats, oFlags, oSlots, oGroups, groupBytes, smemBytes;
@@ -79,10 +79,12 @@ struct TmaTraits {
   static constexpr int PP = P * P, NV = Phys::NV, NT = Phys::NT, NF = Phys::NF;
   static constexpr int TS = trace_side_stride<P, NT, R>();
   static constexpr int TPE = (PP + 31) / 32 * 32;
-  static constexpr int kMaxGroups = 8;
+  static constexpr int kMaxGroups = 9;
   static constexpr int kThreadsMax = 32 + kMaxGroups * TPE;
-  // per-group compute arrays (bulk type)
-  static constexpr int groupBytes = (int)(((NF * PP + 2 * NV * PP + 4 * NV * P) * sizeof(R) + 127) / 128 * 128);
+  // per-group compute arrays (bulk type): the node fields of the updated
+  // solution alias the contravariant flux, then the boundary-normal flux
+  static constexpr int kU = (NF * PP > 2 * NV * PP) ? NF * PP : 2 * NV * PP;
+  static constexpr int groupBytes = (int)(((kU + 4 * NV * P) * sizeof(R) + 127) / 128 * 128);
 };
 
 template <int P, class Phys, typename R>
@@ -92,14 +94,13 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   constexpr int NV = T::NV, NT = T::NT, NF = T::NF, PP = T::PP, TS = T::TS, TPE = T::TPE, N = P - 1;
   constexpr bool kLSW = (NV == 3 && !Phys::kLaggedVelocity);
   constexpr bool kSW = Phys::kLaggedVelocity;
-  constexpr bool kCIG = (NV == 4);
   extern __shared__ __align__(128) unsigned char smem[];
   const int C = pl.groups;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + 2 * C;
   double* sdg = reinterpret_cast<double*>(smem + pl.oMats);
   double* sb = sdg + PP;
-  double* srw = sb + 2 * P;
+  double* sqw = sb + 2 * P;
   volatile int* gflag = reinterpret_cast<volatile int*>(smem + pl.oFlags);
   unsigned char* slots = smem + pl.oSlots;
 
@@ -112,7 +113,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   }
   for (int k = threadIdx.x; k < PP; k += blockDim.x) sdg[k] = a.dgM[k];
   for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) sb[k] = a.bM[k];
-  for (int k = threadIdx.x; k < P; k += blockDim.x) srw[k] = a.qw[k];
+  for (int k = threadIdx.x; k < P; k += blockDim.x) sqw[k] = a.qw[k];
   __syncthreads();
 
   const long long nMine =
@@ -125,12 +126,23 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     const int lane = threadIdx.x & 31;
     bool abort = false;
     long long issued = 0;
+    const R* trIn = reinterpret_cast<const R*>(a.trIn);
+    const R* vIn = reinterpret_cast<const R*>(a.velIn);
     for (long long k0 = 0; k0 < nMine && !abort; k0 += 32) {
       // each lane fetches the connectivity of one element of this batch
       int nbE[4] = {0, 0, 0, 0}, nbS[4] = {0, 0, 0, 0};  // e2 (1-based, 0 = none), s2 (0-based)
       if (k0 + lane < nMine) {
         const long long e = blockIdx.x + (k0 + lane) * gridDim.x;
-        const int* si = a.sideInfo + 20 * e;
+        const int4* si4 = reinterpret_cast<const int4*>(a.sideInfo + 20 * e);
+        int si[20];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          const int4 v = si4[q];
+          si[4 * q] = v.x;
+          si[4 * q + 1] = v.y;
+          si[4 * q + 2] = v.z;
+          si[4 * q + 3] = v.w;
+        }
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
           if (si[5 * s + 4] == 0) {
@@ -160,16 +172,13 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
             unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
             uint64_t* bar = &full[2 * g + buf];
             const uint32_t qb = NV * PP * 8;
-            uint32_t bytes = qb + 4 * PP * 8 + PP * 8 + 8 * P * 8 + 4 * P * 8 + 80;
-            if (rk) bytes += qb;
             const uint32_t tsb = TS * sizeof(R);
             const uint32_t vnb = 2 * P * sizeof(R);
             int nInt = 0;
 #pragma unroll
             for (int s = 0; s < 4; ++s) nInt += (e2[s] != 0);
-            bytes += nInt * tsb;
+            uint32_t bytes = qb + 4 * PP * 8 + 8 * P * 8 + 4 * P * 8 + 80 + 4 * tsb + nInt * tsb;
             if constexpr (kSW) bytes += 8 * P * sizeof(R) + nInt * vnb;
-            // model fields
             uint32_t xb[5] = {0, 0, 0, 0, 0};
             if constexpr (kLSW) {
               xb[0] = PP * 8;
@@ -187,19 +196,16 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
             mbar_arrive_expect_tx(bar, bytes);
             if (!(a.debugStarve && blockIdx.x == 0 && k == 0)) {
               bulk_g2s(sl + pl.oQ, a.q + (size_t)e * NV * PP, qb, bar);
-              if (rk) bulk_g2s(sl + pl.oG, a.G + (size_t)e * NV * PP, qb, bar);
               bulk_g2s(sl + pl.oDsdx, a.dsdx + (size_t)e * 4 * PP, 4 * PP * 8, bar);
-              bulk_g2s(sl + pl.oJ, a.J + (size_t)e * PP, PP * 8, bar);
               bulk_g2s(sl + pl.oNhat, a.nHat + (size_t)e * 8 * P, 8 * P * 8, bar);
               bulk_g2s(sl + pl.oNs, a.nScale + (size_t)e * 4 * P, 4 * P * 8, bar);
               bulk_g2s(sl + pl.oSi, a.sideInfo + (size_t)e * 20, 80, bar);
-              const R* trIn = reinterpret_cast<const R*>(a.trIn);
+              bulk_g2s(sl + pl.oOwn, trIn + (size_t)4 * TS * e, 4 * tsb, bar);
 #pragma unroll
               for (int s = 0; s < 4; ++s)
                 if (e2[s] != 0)
                   bulk_g2s(sl + pl.oNbr + s * tsb, trIn + (size_t)TS * (s2[s] + 4 * (size_t)(e2[s] - 1)), tsb, bar);
               if constexpr (kSW) {
-                const R* vIn = reinterpret_cast<const R*>(a.velIn);
                 bulk_g2s(sl + pl.oVelOwn, vIn + (size_t)e * 8 * P, 8 * P * sizeof(R), bar);
 #pragma unroll
                 for (int s = 0; s < 4; ++s)
@@ -248,9 +254,8 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   const int barId = 1 + g;
   const bool active = t < PP;
   const int i = t % P, j = t / P;
-  R* gfld = reinterpret_cast<R*>(smem + pl.oGroups + (size_t)g * pl.groupBytes);  // [NF][PP]
-  R* gFc = gfld + NF * PP;                                                          // [2][NV][PP]
-  R* gfb = gFc + 2 * NV * PP;                                                       // [4][NV][P]
+  R* gU = reinterpret_cast<R*>(smem + pl.oGroups + (size_t)g * pl.groupBytes);  // Fc [2][NV][PP], later fld [NF][PP]
+  R* gfb = gU + T::kU;                                                            // [4][NV][P]
   R* trOut = reinterpret_cast<R*>(a.trOut);
 
   for (long long jj = 0;; ++jj) {
@@ -260,40 +265,52 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     const int buf = (int)(jj & 1);
     const uint32_t par = (uint32_t)((jj >> 1) & 1);
     const unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
+    // RK register and Jacobian straight from global memory; they are first
+    // used after the face phase, which hides the latency.
+    double Gv[NV], Jij = 1.0;
+    if (active) {
+      Jij = a.J[t + (size_t)PP * e];
+      if (rk) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Gv[v] = a.G[t + (size_t)PP * (v + NV * (size_t)e)];
+      }
+    }
     if (t == 0) gflag[g] = mbar_wait(&full[2 * g + buf], par, a.waitCycles) ? 1 : 0;
     named_bar(barId, TPE);
     if (!gflag[g]) {
       if (t == 0 && a.err) atomicExch(a.err, 1);
       break;
     }
-    const double* sq = reinterpret_cast<const double*>(sl + pl.oQ);
     const int* ssi = reinterpret_cast<const int*>(sl + pl.oSi);
 
-    // ---- A: solution, auxiliaries, contravariant flux
+    // ---- A: solution (kept in registers), flux auxiliaries, contravariant flux
+    double qv[NV];
     R f[NF];
     double na[3] = {0.0, 0.0, 0.0};
     if (active) {
+      const double* sq = reinterpret_cast<const double*>(sl + pl.oQ);
 #pragma unroll
-      for (int v = 0; v < NV; ++v) f[v] = (R)sq[t + PP * v];
-      Phys::template node<R>(f, a);
-#pragma unroll
-      for (int v = 0; v < NF; ++v) gfld[v * PP + t] = f[v];
+      for (int v = 0; v < NV; ++v) {
+        qv[v] = sq[t + PP * v];
+        f[v] = (R)qv[v];
+      }
+      Phys::template node_flux<R>(f, a);
       if constexpr (kLSW) {
         na[0] = reinterpret_cast<const double*>(sl + pl.oX[0])[t];
-        if (pl.oX[2] >= 0 && a.fld[2]) na[1] = reinterpret_cast<const double*>(sl + pl.oX[2])[t];
+        if (pl.oX[2] >= 0) na[1] = reinterpret_cast<const double*>(sl + pl.oX[2])[t];
       } else if constexpr (kSW) {
-        if (a.fld[1]) {
+        if (pl.oX[1] >= 0) {
           const double* gg = reinterpret_cast<const double*>(sl + pl.oX[1]);
           na[0] = gg[2 * t];
           na[1] = gg[2 * t + 1];
         }
       } else {
-        if (a.fld[0]) {
+        if (pl.oX[0] >= 0) {
           const double* gg = reinterpret_cast<const double*>(sl + pl.oX[0]);
           na[0] = gg[2 * t];
           na[1] = gg[2 * t + 1];
         }
-        if (a.fld[1]) na[2] = reinterpret_cast<const double*>(sl + pl.oX[1])[t];
+        if (pl.oX[1] >= 0) na[2] = reinterpret_cast<const double*>(sl + pl.oX[1])[t];
       }
       R Fx[NV], Fy[NV];
       Phys::template flux<R>(f, na, a, Fx, Fy);
@@ -301,24 +318,24 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       const double2 c1 = gp[0], c2 = gp[1];
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        gFc[v * PP + t] = (R)c1.x * Fx[v] + (R)c1.y * Fy[v];
-        gFc[(NV + v) * PP + t] = (R)c2.x * Fx[v] + (R)c2.y * Fy[v];
+        gU[v * PP + t] = (R)c1.x * Fx[v] + (R)c1.y * Fy[v];
+        gU[(NV + v) * PP + t] = (R)c2.x * Fx[v] + (R)c2.y * Fy[v];
       }
     }
-    named_bar(barId, TPE);
 
-    // ---- C: faces (own traces interpolated here, exterior from the buffer)
+    // ---- C: faces; own traces of this stage's solution come from the cache
     if (t < 4 * P) {
       const int s1 = t / P, ii = t % P;
       const int bcid = ssi[5 * s1 + 4];
       const bool physical = (bcid != 0) && (ssi[5 * s1 + 2] == 0);
       const int flip = ssi[5 * s1 + 3] % 10;
-      const R* nbr = reinterpret_cast<const R*>(sl + pl.oNbr + s1 * TS * sizeof(R));
+      const R* own = reinterpret_cast<const R*>(sl + pl.oOwn) + s1 * TS;
+      const R* nbr = reinterpret_cast<const R*>(sl + pl.oNbr) + s1 * TS;
       const int i2 = flip ? N - ii : ii;
       R L[NT], X[NT];
 #pragma unroll
       for (int kf = 0; kf < NT; ++kf) {
-        L[kf] = face_trace<P, R>(gfld + kf * PP, sb, s1, ii);
+        L[kf] = own[ii + P * kf];
         X[kf] = (bcid == 0) ? nbr[i2 + P * kf] : (R)0;
       }
       const double2 nh = reinterpret_cast<const double2*>(sl + pl.oNhat)[ii + P * s1];
@@ -327,9 +344,9 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       if constexpr (kLSW) {
         fx[0] = reinterpret_cast<const double*>(sl + pl.oX[1])[ii + P * s1];
       } else if constexpr (kSW) {
-        if (physical && a.fld[0]) fx[0] = reinterpret_cast<const double*>(sl + pl.oX[0])[ii + P * s1];
+        if (physical && pl.oX[0] >= 0) fx[0] = reinterpret_cast<const double*>(sl + pl.oX[0])[ii + P * s1];
       } else {
-        if (physical && a.fld[2]) {
+        if (physical && pl.oX[2] >= 0) {
           const double* ps = reinterpret_cast<const double*>(sl + pl.oX[2]);
           const double* pp = reinterpret_cast<const double*>(sl + pl.oX[3]);
           const double* pd = reinterpret_cast<const double*>(sl + pl.oX[4]);
@@ -361,51 +378,57 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
 #pragma unroll
       for (int v = 0; v < NV; ++v) gfb[(s1 * NV + v) * P + ii] = out[v];
     }
-    named_bar(barId, TPE);
+    named_bar(barId, TPE);  // flux and face values ready; this buffer is no longer read
+    if (t == 0) mbar_arrive(&empty[2 * g + buf]);
 
     // ---- D: weak divergence + lift, 1/J, source, RK update
+    double dsdt[NV];
     if (active) {
       R Src[NV];
       Phys::template source<R>(f, na, a, Src);
-      const double Jij = reinterpret_cast<const double*>(sl + pl.oJ)[t];
-      const double* sG = reinterpret_cast<const double*>(sl + pl.oG);
-      const R wi = (R)srw[i], wj = (R)srw[j];
+      const R wi = (R)sqw[i], wj = (R)sqw[j];
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        const R* F1 = gFc + v * PP;
-        const R* F2 = gFc + (NV + v) * PP;
+        const R* F1 = gU + v * PP;
+        const R* F2 = gU + (NV + v) * PP;
         R d = (R)0;
 #pragma unroll
         for (int m = 0; m < P; ++m) d = d + (R)sdg[m + P * i] * F1[m + P * j] + (R)sdg[m + P * j] * F2[i + P * m];
         d = d + ((R)sb[i + P] * gfb[(1 * NV + v) * P + j] + (R)sb[i] * gfb[(3 * NV + v) * P + j]) / wi +
             ((R)sb[j + P] * gfb[(2 * NV + v) * P + i] + (R)sb[j] * gfb[(0 * NV + v) * P + i]) / wj;
-        const double dsdt = (double)Src[v] - (double)d / Jij;
-        const size_t gi = t + (size_t)PP * (v + NV * (size_t)e);
-        if (rk) {
-          const double Gn = a.rk_a * sG[t + PP * v] + dsdt;
-          a.G[gi] = Gn;
-          const double qn = sq[t + PP * v] + a.rk_gdt * Gn;
-          a.q[gi] = qn;
-          f[v] = (R)qn;
-        } else {
-          a.dSdt[gi] = dsdt;
-        }
-      }
-      if (rk) {
-        Phys::template node<R>(f, a);
-#pragma unroll
-        for (int v = 0; v < NF; ++v) gfld[v * PP + t] = f[v];
+        dsdt[v] = (double)Src[v] - (double)d / Jij;
       }
     }
-    named_bar(barId, TPE);  // every read of this buffer is done
-    if (t == 0) mbar_arrive(&empty[2 * g + buf]);
+    if (!rk) {
+      if (active)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) a.dSdt[t + (size_t)PP * (v + NV * (size_t)e)] = dsdt[v];
+      named_bar(barId, TPE);  // the flux array is free before the next element writes it
+      continue;
+    }
+    named_bar(barId, TPE);  // every thread is done reading the flux array
+    if (active) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const size_t gi = t + (size_t)PP * (v + NV * (size_t)e);
+        const double Gn = a.rk_a * Gv[v] + dsdt[v];
+        a.G[gi] = Gn;
+        const double qn = qv[v] + a.rk_gdt * Gn;
+        a.q[gi] = qn;
+        f[v] = (R)qn;
+      }
+      Phys::template node<R>(f, a);
+#pragma unroll
+      for (int v = 0; v < NF; ++v) gU[v * PP + t] = f[v];
+    }
+    named_bar(barId, TPE);
 
     // ---- E: traces of the updated solution -> trace cache
-    if (rk) {
+    {
       R* o = trOut + (size_t)4 * TS * e;
       for (int kk = t; kk < 4 * NT * P; kk += TPE) {
         const int ii = kk % P, fs = kk / P, fi = fs % NT, s1 = fs / NT;
-        o[ii + P * fi + TS * s1] = face_trace<P, R>(gfld + fi * PP, sb, s1, ii);
+        o[ii + P * fi + TS * s1] = face_trace_uniform<P, R>(gU + fi * PP, sb, s1, ii);
       }
     }
     named_bar(barId, TPE);
@@ -427,12 +450,11 @@ inline bool make_tma_plan(const StageArgs& a, int smemLimit, TmaPlan& pl) {
     return at;
   };
   pl.oQ = put(NV * PP * 8);
-  pl.oG = put(NV * PP * 8);
   pl.oDsdx = put(4 * PP * 8);
-  pl.oJ = put(PP * 8);
   pl.oNhat = put(8 * P * 8);
   pl.oNs = put(4 * P * 8);
   pl.oSi = put(80);
+  pl.oOwn = put(4 * TS * (int)sizeof(R));
   pl.oNbr = put(4 * TS * (int)sizeof(R));
   for (int x = 0; x < 5; ++x) pl.oX[x] = -1;
   pl.oVelOwn = pl.oVelNbr = -1;
