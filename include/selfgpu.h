@@ -309,6 +309,32 @@ int selfgpu_model2d_set_kernel(selfgpu_model2d* m, int persistent);
 int selfgpu_model2d_set_wait_limit(selfgpu_model2d* m, long long cycles);
 int selfgpu_model2d_inject_stall(selfgpu_model2d* m, int enable);
 
+/* ========================================= 4. tendency without allocation */
+
+/* Size of the fixed device array behind selfgpu_cig2d_tendency_noalloc. */
+#define SELFGPU_NOALLOC_SCRATCH_BYTES (16 * 1024 * 1024)
+
+/* No counterpart in the reference: an added entry point for callers that may
+ * not allocate device memory (a host code that owns every device buffer and
+ * forbids the library to allocate, a process under a fixed device-memory cap,
+ * a call inside a solver step that must not stall or fail on cudaMalloc).
+ * It computes the CompressibleIdealGas2D tendency dSdt exactly as
+ * selfgpu_model2d_tendency does for a CIG handle with no gravity, drag or
+ * prescribed-boundary fields (periodic or no-normal-flow sides), from
+ * caller-owned device arrays in SELF's layouts (solution (P,P,4,nEl), dsdx,
+ * J, nHat, nScale, sideInfo on the device plus a host copy of sideInfo for
+ * validation) and host copies of dgMatrix, bMatrix and qWeights.  It calls
+ * no allocator: its face-trace scratch is a file-scope device array of
+ * SELFGPU_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
+ * until exit; inputs needing more (above 7281 elements at N = 7, 14563 at
+ * N = 3) are rejected with SELFGPU_ERR_ARG.  The first call on a device looks
+ * up the array's address (make it before any stream capture).  All calls on
+ * a device share the array: calls that overlap on the GPU race. */
+int selfgpu_cig2d_tendency_noalloc(const double* solution, double* dSdt, const double* dsdx, const double* J,
+                                   const double* nHat, const double* nScale, const int* sideInfo_d,
+                                   const int* sideInfo_h, const double* dgMatrix, const double* bMatrix,
+                                   const double* qWeights, double expansionFactor, int N, int nEl, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

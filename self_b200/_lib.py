@@ -45,6 +45,7 @@ _SIGS = {
     "selfgpu_model2d_set_kernel": (c_int, [c_void_p, c_int]),
     "selfgpu_model2d_set_wait_limit": (c_int, [c_void_p, c_longlong]),
     "selfgpu_model2d_inject_stall": (c_int, [c_void_p, c_int]),
+    "selfgpu_cig2d_tendency_noalloc": (c_int, [c_void_p] * 11 + [c_double, c_int, c_int, c_void_p]),
     # drop-in wrappers (src/hip/*.cpp, src/models/hip/*.cpp of the reference)
     "ScalarGridInterp_2D_gpu_wrapper": (None, [PP, PP, PP, c_int, c_int, c_int, c_int]),
     "VectorGridInterp_2D_gpu_wrapper": (None, [PP, PP, PP, c_int, c_int, c_int, c_int]),
