@@ -163,6 +163,46 @@ def cpu_baseline(seconds=12.0, max_steps=STEPS_PER_SOLVE):
                       f"{el:.1f} s, C++ restatement of the reference CPU branches, OpenMP over elements"}
 
 
+def run_forms(steps=20, err_steps=500, n_instances=256):
+    """The ensemble workload: 256 seeded nonlinear ShallowWater instances
+    (nx, ny ~ U{8..64}, N ~ U{3,5,7}, 4-Gaussian topography, reflecting walls,
+    per-instance CFL-0.5 time step), advanced (a) one FP64 handle per instance,
+    (b) batched per degree in FP64, (c) batched per degree in the FP32-bulk form;
+    DOF-updates/s over `steps` RK3 steps each, and the FP32-bulk error against
+    the batched FP64 run after `err_steps` steps (the workload's length)."""
+    import torch
+
+    import self_b200 as S
+    from self_b200 import ensemble as E
+    inst = E.make_instances(n_instances, seed=0)
+    e64 = E.ShallowWaterEnsemble(inst, form=S.FP64, autotune=True)
+    e32 = E.ShallowWaterEnsemble(inst, form=S.FP32_BULK, autotune=True)
+    un = E.UnbatchedShallowWater(inst)
+    dof = sum(i.dof() for i in inst)
+    out = {"workload": f"{n_instances} ShallowWater instances, nx,ny~U{{8..64}}, N~U{{3,5,7}}, FP32/FP64, "
+                       f"per-instance CFL 0.5; rates over {steps} RK3 steps", "dof": dof}
+    for name, runner in (("unbatched_fp64", un), ("batched_fp64", e64), ("batched_fp32_bulk", e32)):
+        runner.reset()
+        runner.ForwardStep(2)
+        torch.cuda.synchronize()
+        l0 = runner.launches() if hasattr(runner, "launches") else None
+        t = E.time_it(lambda: runner.ForwardStep(steps))
+        out[name] = {"value": dof * steps / t, "unit": "DOF-updates/s", "ms_per_rk3_step": 1e3 * t / steps}
+    out["speedup_fp32_batched_vs_unbatched_fp64"] = out["batched_fp32_bulk"]["value"] / out["unbatched_fp64"]["value"]
+    out["autotune"] = {f"N={k}": v for k, v in e32.tuning.items()}
+    e64.reset()
+    e32.reset()
+    e64.ForwardStep(err_steps)
+    e32.ForwardStep(err_steps)
+    torch.cuda.synchronize()
+    worst = 0.0
+    for it in inst:
+        a, b = e32.solution(it), e64.solution(it)
+        worst = max(worst, float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)))
+    out["fp32_bulk_rel_l2_err_vs_fp64_after_%d_steps" % err_steps] = worst
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -318,6 +358,8 @@ def run_engine(args, rank, world, local_rank):
                                 "k_fused_stage<8,PhysCIG,double>") + " (one RK stage over all elements)"},
         "clocks": clk,
     }
+    if not args.no_forms:
+        line["forms"] = run_forms()
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     print(json.dumps(line), flush=True)
@@ -330,6 +372,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="selfgpu", choices=["selfgpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the ensemble / FP32-bulk form measurements")
     ap.add_argument("--kernel", default="persistent", choices=["persistent", "per-element"],
                     help="stage kernel: persistent bulk-copy kernel or one CTA per element group")
     args = ap.parse_args()

@@ -263,6 +263,9 @@ int selfgpu_model2d_set_state(selfgpu_model2d* m, double* solution, double* work
  *  CIG: "environmentalsGradient" (2,P,P,2,nEl), "environmentals" (P,P,2,nEl),
  *       "prescribedSolution.boundary", "prescribedPrimitive.boundary",
  *       "prescribedDiagnostics.boundary" (P,4,4,nEl each)
+ *  any: "elementDt" (nEl) -- a time step per element, used by
+ *       selfgpu_model2d_rk3 instead of its dt argument (ensembles of
+ *       independent instances batched into one handle)
  * A field never set reads as zero. */
 int selfgpu_model2d_set_field(selfgpu_model2d* m, const char* name, const double* ptr);
 
@@ -299,6 +302,13 @@ long long selfgpu_model2d_persistent_launch_count(const selfgpu_model2d* m);
  * wherever it applies (even P, 16-byte aligned buffers); 0 forces the
  * one-CTA-per-element-group kernel. */
 int selfgpu_model2d_set_kernel(selfgpu_model2d* m, int persistent);
+
+/* Autotuner: times the per-element-group kernel and the persistent kernel at
+ * every consumer-group count that fits (elements in flight per CTA, each with
+ * its double-buffered staging tile) on tendency launches over this handle's
+ * own data, keeps the fastest, and reports it (persistent 0/1, group count,
+ * microseconds per stage).  Allocates a temporary dSdt buffer. */
+int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, float* usPerStage);
 
 /* Failure detection.  Every wait inside the persistent kernel is bounded; a
  * wait that runs out sets an error word, the kernel stops and returns, and the

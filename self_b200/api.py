@@ -190,6 +190,9 @@ class Model2D:
         check(lib().selfgpu_model2d_set_params(self._h, self.g, self.fCori, self.expansionFactor, self.R))
 
     def _set_field(self, name, tensor):
+        # Set-up fields are produced by drop-in wrappers on the legacy default
+        # stream; finish them before a handle on another stream can read them.
+        torch.cuda.synchronize()
         self._fields[name] = tensor
         check(lib().selfgpu_model2d_set_field(self._h, name.encode(), None if tensor is None else _ptr(tensor)))
 

@@ -50,7 +50,7 @@ struct selfgpu_model2d {
   int* derr = nullptr;  // error word of the persistent kernel's bounded waits
   long long launches = 0;
   long long tmaLaunches = 0;
-  StageLaunch cfg{true, 0, 148};
+  StageLaunch cfg{true, 0, 148, 0};
   // graph cache: one captured RK step per starting buffer parity
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   long long graphTma[2][2] = {{0, 0}, {0, 0}};
@@ -95,6 +95,7 @@ struct selfgpu_model2d {
       a.mode = MODE_RK;
       a.rk_a = kRK3a[m];
       a.rk_gdt = kRK3g[m] * dt;
+      a.rk_g = kRK3g[m];
       a.trIn = tr[cur];
       a.trOut = tr[1 - cur];
       if (model == SELFGPU_MODEL_SW) {
@@ -147,7 +148,11 @@ int selfgpu_model2d_create(selfgpu_model2d** out, int model, int N, int nEl, int
     }
     m->ownStream = true;
   }
-  const size_t trBytes = (size_t)m->P * nt_of(model) * 4 * nEl * m->elemBytes();
+  // one (element, side) block holds NT fields x P nodes, padded to 16 bytes
+  // (trace_side_stride in fused_stage.cuh)
+  const size_t per16 = 16 / m->elemBytes();
+  const size_t ts = ((size_t)nt_of(model) * m->P + per16 - 1) / per16 * per16;
+  const size_t trBytes = ts * 4 * (size_t)nEl * m->elemBytes();
   for (int k = 0; k < 2; ++k) {
     e = cudaMalloc(&m->tr[k], trBytes);
     if (e == cudaSuccess && model == SELFGPU_MODEL_SW) e = cudaMalloc(&m->vel[k], (size_t)m->P * 2 * 4 * nEl * m->elemBytes());
@@ -233,6 +238,11 @@ int selfgpu_model2d_set_state(selfgpu_model2d* m, double* solution, double* work
 int selfgpu_model2d_set_field(selfgpu_model2d* m, const char* name, const double* ptr) {
   if (!m || !name) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_field: null argument");
   const std::string n(name);
+  if (n == "elementDt") {  // per-element time step (nEl doubles); replaces dt in selfgpu_model2d_rk3
+    m->base.dtElem = ptr;
+    m->drop_graphs();
+    return SELFGPU_OK;
+  }
   int slot = -1;
   if (m->model == SELFGPU_MODEL_LSW) {
     if (n == "H") slot = 0;
@@ -401,6 +411,80 @@ int selfgpu_model2d_set_kernel(selfgpu_model2d* m, int persistent) {
 }
 
 long long selfgpu_model2d_persistent_launch_count(const selfgpu_model2d* m) { return m ? m->tmaLaunches : 0; }
+
+int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, float* usPerStage) {
+  int rc = check_ready(m, "selfgpu_model2d_autotune");
+  if (rc) return rc;
+  // Candidates: the per-element-group kernel and the persistent kernel with
+  // every consumer-group count from 2 up to what fits.  Each is timed on
+  // tendency launches (the state is not modified) over the handle's data.
+  const size_t n = (size_t)m->P * m->P * nv_of(m->model) * m->nEl;
+  double* scratch = nullptr;
+  cudaError_t e = cudaMalloc(&scratch, n * sizeof(double));
+  if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_autotune", e);
+  if (!m->valid) {
+    e = m->prologue();
+    if (e != cudaSuccess) {
+      cudaFree(scratch);
+      return fail_cuda("selfgpu_model2d_autotune", e);
+    }
+  }
+  StageArgs a = m->base;
+  a.mode = MODE_TENDENCY;
+  a.dSdt = scratch;
+  a.trIn = m->tr[m->cur];
+  a.trOut = nullptr;
+  if (m->model == SELFGPU_MODEL_SW) {
+    a.velIn = m->vel[m->vcur];
+    a.velOut = m->vel[1 - m->vcur];  // written, not consumed: the cache parity is left unchanged
+  }
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  const StageLaunch saved = m->cfg;
+  float best = 1e30f;
+  StageLaunch bestCfg = saved;
+  for (int cand = 0; cand <= 8; ++cand) {
+    StageLaunch c = saved;
+    if (cand == 0) {
+      c.allowTma = false;
+    } else {
+      c.allowTma = true;
+      c.maxGroups = cand + 1;  // 2..9 consumer groups, capped by what fits
+    }
+    m->cfg = c;
+    int tma = 0;
+    e = (m->form == SELFGPU_FP64) ? launch_stage_fp64(m->model, m->P, a, c, m->stream, &tma)
+                                  : launch_stage_fp32(m->model, m->P, a, c, m->stream, &tma);
+    if (e != cudaSuccess) break;
+    if (cand > 0 && !tma) break;  // the persistent kernel does not apply
+    cudaEventRecord(t0, m->stream);
+    for (int r = 0; r < 3; ++r)
+      (m->form == SELFGPU_FP64) ? launch_stage_fp64(m->model, m->P, a, c, m->stream, &tma)
+                                : launch_stage_fp32(m->model, m->P, a, c, m->stream, &tma);
+    cudaEventRecord(t1, m->stream);
+    cudaEventSynchronize(t1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    if (ms < best) {
+      best = ms;
+      bestCfg = c;
+    }
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  cudaFree(scratch);
+  if (e != cudaSuccess) {
+    m->cfg = saved;
+    return fail_cuda("selfgpu_model2d_autotune", e);
+  }
+  m->cfg = bestCfg;
+  m->drop_graphs();
+  if (persistent) *persistent = bestCfg.allowTma ? 1 : 0;
+  if (groups) *groups = bestCfg.allowTma ? bestCfg.maxGroups : 0;
+  if (usPerStage) *usPerStage = best * 1000.f / 3.f;
+  return SELFGPU_OK;
+}
 
 int selfgpu_model2d_check_finite(selfgpu_model2d* m) {
   if (!m || !m->haveState) return set_error(SELFGPU_ERR_STATE, "selfgpu_model2d_check_finite: no state bound");

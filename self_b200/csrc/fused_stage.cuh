@@ -62,8 +62,10 @@ struct StageArgs {
   // model parameters and fields (FP64, caller owned; NULL = absent)
   double g, fC, gamma, Rgas;
   const double* fld[5];
-  // RK coefficients: G = a G + dSdt ; q = q + gdt G
-  double rk_a, rk_gdt;
+  // RK coefficients: G = a G + dSdt ; q = q + gdt G, with gdt = rk_gdt, or
+  // rk_g * dtElem[e] when a per-element time step is bound (ensembles)
+  double rk_a, rk_gdt, rk_g;
+  const double* dtElem;
   // bounded waits of the persistent kernel (clock cycles) and its error word
   long long waitCycles;
   int* err;
@@ -401,38 +403,40 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
         sm.own[s1][fi][ii] = face_trace<P, R>(sm.fld[fi], sb, s1, ii);
       }
     __syncthreads();
-    if (live && t < 4 * P) {
-      const int s1 = t / P, ii = t % P;
-      const int* si = a.sideInfo + 5 * (s1 + 4 * e);
-      const int bcid = si[4];
-      const bool physical = (bcid != 0) && (si[2] == 0);
-      R L[NT], X[NT];
+    // 4P face nodes per element; for P <= 3 there are fewer node threads (P*P)
+    if (live)
+      for (int k = t; k < 4 * P; k += PP) {
+        const int s1 = k / P, ii = k % P;
+        const int* si = a.sideInfo + 5 * (s1 + 4 * e);
+        const int bcid = si[4];
+        const bool physical = (bcid != 0) && (si[2] == 0);
+        R L[NT], X[NT];
 #pragma unroll
-      for (int k = 0; k < NT; ++k) {
-        L[k] = sm.own[s1][k][ii];
-        X[k] = (bcid == 0) ? sm.ext[s1][k][ii] : (R)0;
-      }
-      const long long gface = ii + (long long)P * (s1 + 4 * e);
-      const double2 nh = reinterpret_cast<const double2*>(a.nHat)[gface];
-      const double ns = a.nScale[gface];
-      double fx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-      if (physical) face_aux_global<Phys>(a, s1, ii, e, P, fx);
-      else if constexpr (Phys::NV == 3 && !Phys::kLaggedVelocity) face_aux_global<Phys>(a, s1, ii, e, P, fx);
-      R velL[2] = {(R)0, (R)0}, velR[2] = {(R)0, (R)0};
-      if constexpr (Phys::kLaggedVelocity) {
-        velL[0] = sm.vel[0][s1][0][ii];
-        velL[1] = sm.vel[0][s1][1][ii];
-        velR[0] = sm.vel[1][s1][0][ii];
-        velR[1] = sm.vel[1][s1][1][ii];
-        R* vOut = reinterpret_cast<R*>(a.velOut);  // read by the next stage
-        vOut[ii + P * (0 + 2 * (s1 + 4 * e))] = L[0] / L[2];
-        vOut[ii + P * (1 + 2 * (s1 + 4 * e))] = L[1] / L[2];
-      }
-      R out[NV];
-      Phys::template face<R>(bcid, physical, L, X, velL, velR, nh.x, nh.y, ns, fx, a, out);
+        for (int m = 0; m < NT; ++m) {
+          L[m] = sm.own[s1][m][ii];
+          X[m] = (bcid == 0) ? sm.ext[s1][m][ii] : (R)0;
+        }
+        const long long gface = ii + (long long)P * (s1 + 4 * e);
+        const double2 nh = reinterpret_cast<const double2*>(a.nHat)[gface];
+        const double ns = a.nScale[gface];
+        double fx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (physical) face_aux_global<Phys>(a, s1, ii, e, P, fx);
+        else if constexpr (Phys::NV == 3 && !Phys::kLaggedVelocity) face_aux_global<Phys>(a, s1, ii, e, P, fx);
+        R velL[2] = {(R)0, (R)0}, velR[2] = {(R)0, (R)0};
+        if constexpr (Phys::kLaggedVelocity) {
+          velL[0] = sm.vel[0][s1][0][ii];
+          velL[1] = sm.vel[0][s1][1][ii];
+          velR[0] = sm.vel[1][s1][0][ii];
+          velR[1] = sm.vel[1][s1][1][ii];
+          R* vOut = reinterpret_cast<R*>(a.velOut);  // read by the next stage
+          vOut[ii + P * (0 + 2 * (s1 + 4 * e))] = L[0] / L[2];
+          vOut[ii + P * (1 + 2 * (s1 + 4 * e))] = L[1] / L[2];
+        }
+        R out[NV];
+        Phys::template face<R>(bcid, physical, L, X, velL, velR, nh.x, nh.y, ns, fx, a, out);
 #pragma unroll
-      for (int v = 0; v < NV; ++v) sm.fb[s1][v][ii] = out[v];
-    }
+        for (int v = 0; v < NV; ++v) sm.fb[s1][v][ii] = out[v];
+      }
     __syncthreads();
     if (live) {
       R f[NF];
@@ -440,8 +444,11 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
       for (int v = 0; v < NF; ++v) f[v] = sm.fld[v][t];
       double na[3];
       node_aux_global<Phys>(a, t, e, PP, na);
-      R Src[NV];
-      Phys::template source<R>(f, na, a, Src);
+      // sources in FP64 in every form (well-balanced topography / gravity terms)
+      double qd[NV], Src[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) qd[v] = a.q[t + (long long)PP * (v + NV * e)];
+      Phys::template source<double>(qd, na, a, Src);
       const double Jij = a.J[gnode];
       const R wi = (R)srw[i], wj = (R)srw[j];
 #pragma unroll
@@ -452,14 +459,14 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
           d = d + (R)sdg[m + P * i] * sm.Fc[0][v][m + P * j] + (R)sdg[m + P * j] * sm.Fc[1][v][i + P * m];
         d = d + ((R)sb[i + P] * sm.fb[1][v][j] + (R)sb[i] * sm.fb[3][v][j]) / wi +
             ((R)sb[j + P] * sm.fb[2][v][i] + (R)sb[j] * sm.fb[0][v][i]) / wj;
-        const double dsdt = (double)Src[v] - (double)d / Jij;
+        const double dsdt = Src[v] - (double)d / Jij;
         const long long gi = t + (long long)PP * (v + NV * e);
         if (a.mode == MODE_TENDENCY) {
           a.dSdt[gi] = dsdt;
         } else {
           const double Gn = a.rk_a * a.G[gi] + dsdt;
           a.G[gi] = Gn;
-          const double qn = a.q[gi] + a.rk_gdt * Gn;
+          const double qn = qd[v] + (a.dtElem ? a.rk_g * a.dtElem[e] : a.rk_gdt) * Gn;
           a.q[gi] = qn;
           f[v] = (R)qn;
         }
@@ -486,13 +493,14 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
     // solution (SetSolution leaves solution%boundary = BoundaryInterp(solution)).
     if (a.mode == MODE_TRACES && a.velOut != nullptr) {
       __syncthreads();
-      if (live && t < 4 * P) {
-        const int s1 = t / P, ii = t % P;
-        R* vOut = reinterpret_cast<R*>(a.velOut);
-        const R H = o[ii + P * 2 + TS * s1];
-        vOut[ii + P * (0 + 2 * (s1 + 4 * e))] = o[ii + P * 0 + TS * s1] / H;
-        vOut[ii + P * (1 + 2 * (s1 + 4 * e))] = o[ii + P * 1 + TS * s1] / H;
-      }
+      if (live)
+        for (int k = t; k < 4 * P; k += PP) {
+          const int s1 = k / P, ii = k % P;
+          R* vOut = reinterpret_cast<R*>(a.velOut);
+          const R H = o[ii + P * 2 + TS * s1];
+          vOut[ii + P * (0 + 2 * (s1 + 4 * e))] = o[ii + P * 0 + TS * s1] / H;
+          vOut[ii + P * (1 + 2 * (s1 + 4 * e))] = o[ii + P * 1 + TS * s1] / H;
+        }
     }
   }
 }

@@ -79,6 +79,7 @@ struct TmaTraits {
   static constexpr int PP = P * P, NV = Phys::NV, NT = Phys::NT, NF = Phys::NF;
   static constexpr int TS = trace_side_stride<P, NT, R>();
   static constexpr int TPE = (PP + 31) / 32 * 32;
+  static_assert(TPE >= 4 * P, "the face phase gives each of the 4P face nodes its own thread");
   static constexpr int kMaxGroups = 9;
   static constexpr int kThreadsMax = 32 + kMaxGroups * TPE;
   // per-group compute arrays (bulk type): the node fields of the updated
@@ -384,8 +385,9 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     // ---- D: weak divergence + lift, 1/J, source, RK update
     double dsdt[NV];
     if (active) {
-      R Src[NV];
-      Phys::template source<R>(f, na, a, Src);
+      // sources in FP64 in every form (well-balanced topography / gravity terms)
+      double Src[NV];
+      Phys::template source<double>(qv, na, a, Src);
       const R wi = (R)sqw[i], wj = (R)sqw[j];
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
@@ -396,24 +398,24 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         for (int m = 0; m < P; ++m) d = d + (R)sdg[m + P * i] * F1[m + P * j] + (R)sdg[m + P * j] * F2[i + P * m];
         d = d + ((R)sb[i + P] * gfb[(1 * NV + v) * P + j] + (R)sb[i] * gfb[(3 * NV + v) * P + j]) / wi +
             ((R)sb[j + P] * gfb[(2 * NV + v) * P + i] + (R)sb[j] * gfb[(0 * NV + v) * P + i]) / wj;
-        dsdt[v] = (double)Src[v] - (double)d / Jij;
+        dsdt[v] = Src[v] - (double)d / Jij;
       }
     }
     if (!rk) {
       if (active)
 #pragma unroll
         for (int v = 0; v < NV; ++v) a.dSdt[t + (size_t)PP * (v + NV * (size_t)e)] = dsdt[v];
-      named_bar(barId, TPE);  // the flux array is free before the next element writes it
-      continue;
+      continue;  // the next element's post-wait barrier orders the reuse of the flux array
     }
     named_bar(barId, TPE);  // every thread is done reading the flux array
     if (active) {
+      const double gdt = a.dtElem ? a.rk_g * a.dtElem[e] : a.rk_gdt;
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
         const size_t gi = t + (size_t)PP * (v + NV * (size_t)e);
         const double Gn = a.rk_a * Gv[v] + dsdt[v];
         a.G[gi] = Gn;
-        const double qn = qv[v] + a.rk_gdt * Gn;
+        const double qn = qv[v] + gdt * Gn;
         a.q[gi] = qn;
         f[v] = (R)qn;
       }
@@ -431,13 +433,13 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         o[ii + P * fi + TS * s1] = face_trace_uniform<P, R>(gU + fi * PP, sb, s1, ii);
       }
     }
-    named_bar(barId, TPE);
+    // no barrier here: the next element's post-wait barrier orders the reuse of gU
   }
 }
 
 // Host-side plan for k_fused_stage_tma given the smem budget.
 template <int P, class Phys, typename R>
-inline bool make_tma_plan(const StageArgs& a, int smemLimit, TmaPlan& pl) {
+inline bool make_tma_plan(const StageArgs& a, int smemLimit, TmaPlan& pl, int maxGroups = 0) {
   using T = TmaTraits<P, Phys, R>;
   constexpr int PP = T::PP, NV = T::NV, TS = T::TS;
   constexpr bool kLSW = (NV == 3 && !Phys::kLaggedVelocity);
@@ -475,7 +477,8 @@ inline bool make_tma_plan(const StageArgs& a, int smemLimit, TmaPlan& pl) {
   }
   pl.slotBytes = (o + 127) / 128 * 128;
   pl.groupBytes = T::groupBytes;
-  for (int C = T::kMaxGroups; C >= 1; --C) {
+  const int cMax = (maxGroups > 0 && maxGroups < T::kMaxGroups) ? maxGroups : T::kMaxGroups;
+  for (int C = cMax; C >= 1; --C) {
     int s = 0;
     s += 4 * C * 8;  // barriers
     s = (s + 15) / 16 * 16;

@@ -28,6 +28,7 @@ struct StageLaunch {
   bool allowTma;   // use the persistent bulk-copy kernel where it applies
   int smemOptin;   // opt-in shared memory per block (bytes)
   int numSMs;
+  int maxGroups;   // cap on the persistent kernel's consumer groups (0 = as many as fit)
 };
 }  // namespace selfgpu
 

@@ -32,7 +32,7 @@ cudaError_t launch_one(const StageArgs& a, const StageLaunch& L, cudaStream_t st
               aligned16(a.trIn) && (a.velIn == nullptr || aligned16(a.velIn));
     for (int k = 0; k < 5; ++k) ok = ok && (a.fld[k] == nullptr || aligned16(a.fld[k]));
     TmaPlan pl{};
-    if (ok && make_tma_plan<P, Phys, R>(a, L.smemOptin, pl)) {
+    if (ok && make_tma_plan<P, Phys, R>(a, L.smemOptin, pl, L.maxGroups)) {
       static bool attrSet = false;  // one instantiation per (P, Phys, R)
       if (!attrSet) {
         cudaError_t e = cudaFuncSetAttribute(k_fused_stage_tma<P, Phys, R>,

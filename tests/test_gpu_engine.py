@@ -66,7 +66,7 @@ CASES = [(m, k) for m in ("LSW", "SW", "CIG") for k in ("periodic", "walls", "fl
         [("CIG", "prescribed")]
 
 
-@pytest.mark.parametrize("N", [3, 7])
+@pytest.mark.parametrize("N", [2, 3, 4, 7])  # odd and even P; P*P < 4P at N = 2
 @pytest.mark.parametrize("model,mesh_kind", CASES)
 def test_tendency_matches_oracle(model, mesh_kind, N):
     import self_b200 as S
@@ -100,10 +100,11 @@ def test_fp64_tendency_and_steps_are_bit_exact(model, mesh_kind):
     np.testing.assert_array_equal(S.to_host(mod2.solution).reshape(ref.shape, order="F"), ref)
 
 
+@pytest.mark.parametrize("N", [2, 5])
 @pytest.mark.parametrize("model,mesh_kind", CASES)
-def test_rk3_steps_match_oracle(model, mesh_kind):
+def test_rk3_steps_match_oracle(model, mesh_kind, N):
     import self_b200 as S
-    N, n, dt = 5, 12, 1e-3
+    n, dt = 12, 1e-3
     mod_o, mod, _, _ = build_pair(model, mesh_kind, N, seed=3)
     mod_o.rk3(n, dt)
     mod.ForwardStep(n, dt)
@@ -214,6 +215,39 @@ def test_bounded_wait_timeout_is_reported_and_context_survives():
     mod.ForwardStep(2, 1e-3)
     mod.Sync()
     mod.CheckFinite()
+
+
+@pytest.mark.parametrize("model,mesh_kind,N", [("CIG", "periodic", 7), ("SW", "walls", 5), ("LSW", "walls", 5)])
+def test_fp32_bulk_form_error_vs_fp64_oracle(model, mesh_kind, N, capsys):
+    """FP32-bulk form (float fluxes, traces and divergence; FP64 metrics,
+    sources, 1/J and RK accumulation): relative L2 error against the FP64
+    oracle after 40 RK3 steps on smooth states."""
+    import self_b200 as S
+    kw = C.mesh_kwargs(mesh_kind)
+    om, pm = C.oracle_mesh(kw), C.product_mesh(kw)
+    mod_o = O.Model(C.MODELS[model], N, om)
+    geo_o = O.Geometry(N, om)
+    geo = S.SEMQuad(S.Lagrange(N), pm)
+    cls = {"LSW": S.LinearShallowWater, "SW": S.ShallowWater, "CIG": S.CompressibleIdealGas2D}[model]
+    mod = cls(pm, geo, form=S.FP32_BULK)
+    aux = C.aux_fields(model, geo_o.x, 0)
+    if model == "LSW":
+        mod_o.set("H", aux["H"])
+        mod.SetBathymetry(aux["H"])
+    elif model == "SW":
+        mod_o.set("topography", aux["topography"])
+        mod.SetTopography(aux["topography"])
+    q0 = C.initial_state(model, geo_o.x, 0)
+    mod_o.set("solution", q0)
+    mod.SetSolution(q0)
+    mod_o.rk3(40, 1e-3)
+    mod.ForwardStep(40, 1e-3)
+    ref = mod_o.get("solution", q0.shape)
+    got = S.to_host(mod.solution).reshape(ref.shape, order="F")
+    err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    with capsys.disabled():
+        print(f"\nFP32-bulk {model} N={N}: relative L2 error after 40 steps = {err:.3e}")
+    assert err < 1e-5
 
 
 def test_engine_rejects_malformed_side_info():
