@@ -244,6 +244,7 @@ def run_reference(args, rank, world):
 def run_engine(args, rank, world, local_rank):
     import torch
     import self_b200 as S
+    from self_b200 import replicas as R
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     stream = torch.cuda.Stream(device=dev)
@@ -268,9 +269,6 @@ def run_engine(args, rank, world, local_rank):
         for _ in range(args.warmup):
             solve()
     stream.synchronize()
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
     launches0 = model.LaunchCount()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -279,8 +277,7 @@ def run_engine(args, rank, world, local_rank):
     except Exception:
         smi_id = str(local_rank)
     clocks = Clocks(smi_id)
-    if dist:
-        dist.barrier()
+    R.barrier()
     torch.cuda.synchronize()
     with clocks, torch.cuda.stream(stream):
         for k in range(args.steps):
@@ -289,18 +286,13 @@ def run_engine(args, rank, world, local_rank):
             solve()
             ends[k].record(stream)
         torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    R.barrier()
     ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     launches = model.LaunchCount() - launches0  # fused-stage launches (plus one trace prologue per solve)
     persistent = S.lib().selfgpu_model2d_persistent_launch_count(model._h)
     clk = clocks.summary()
-    t_max = ms
-    if dist:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = world * DOF * STEPS_PER_SOLVE * args.steps / (t_max / 1e3)
+    t_max = R.max_over_ranks(ms)
+    value = R.aggregate_rate(DOF * STEPS_PER_SOLVE * args.steps, world, t_max / 1e3)
     stage_ms = ms / (args.steps * 3 * STEPS_PER_SOLVE)
     per_launch = algorithmic_bytes_per_element_stage() * NEL
     achieved = per_launch / (stage_ms / 1e3) / 1e9
@@ -319,8 +311,7 @@ def run_engine(args, rank, world, local_rank):
             model.ForwardStep(STEPS_PER_SOLVE, dt)
             host_out.copy_(model.solution, non_blocking=True)
         stream.synchronize()
-        if dist:
-            dist.barrier()
+        R.barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
@@ -331,12 +322,8 @@ def run_engine(args, rank, world, local_rank):
             host_out.copy_(model.solution, non_blocking=True)
         e1.record(stream)
         stream.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = world * DOF * STEPS_PER_SOLVE * args.steps / (e2e_ms / 1e3)
+    e2e_ms = R.max_over_ranks(e0.elapsed_time(e1))
+    e2e = R.aggregate_rate(DOF * STEPS_PER_SOLVE * args.steps, world, e2e_ms / 1e3)
     model.CheckFinite()
 
     if rank != 0:
@@ -376,27 +363,15 @@ def main():
     ap.add_argument("--kernel", default="persistent", choices=["persistent", "per-element"],
                     help="stage kernel: persistent bulk-copy kernel or one CTA per element group")
     args = ap.parse_args()
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        backend = "gloo" if args.impl == "reference" else "nccl"
-        if backend == "nccl":
-            import torch
-            torch.cuda.set_device(local_rank)
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    from self_b200 import replicas as R
+    rank, world, local_rank = R.init("gloo" if args.impl == "reference" else "nccl")
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
         else:
             run_engine(args, rank, world, local_rank)
     finally:
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        R.finalize()
 
 
 if __name__ == "__main__":
