@@ -25,6 +25,8 @@
 #ifndef SELFGPU_H
 #define SELFGPU_H
 
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -344,6 +346,67 @@ int selfgpu_cig2d_tendency_noalloc(const double* solution, double* dSdt, const d
                                    const double* nHat, const double* nScale, const int* sideInfo_d,
                                    const int* sideInfo_h, const double* dgMatrix, const double* bMatrix,
                                    const double* qWeights, double expansionFactor, int N, int nEl, void* stream);
+
+/* ==================================== 5. shock closure (artificial viscosity) */
+
+/* No counterpart in the reference's tendency: an artificial-viscosity closure
+ * for CompressibleIdealGas2D built from the reference's operators
+ * (BassiRebaySides + GradientBR, src/SELF_MappedData.f90:919-1078; the
+ * Advection2D diffusive fluxes, src/models/hip/SELF_Advection2D.cpp:66-175)
+ * with one viscosity per element.  With a closure set, every tendency / RK
+ * stage adds div(nu_e grad q) through BR1, one extra launch per stage.
+ *   mode 1: nu_e from the modal-decay indicator of the density (Persson &
+ *           Peraire): a(s) ramps from 0 at s0 - kappa to 1 at s0 + kappa,
+ *           s = log10 of the energy fraction in the highest modes;
+ *   mode 2: a from the closure MLP (selfgpu_model2d_set_mlp; N >= 5), the
+ *           indicator as fallback for features outside the training range;
+ *   mode 0: off.
+ * nu_e = a * c * h_e / N * max(|u| + c_sound), h_e = sqrt(element area).
+ * controlPoints: the P quadrature nodes (Lagrange%controlPoints). */
+#define SELFGPU_CLOSURE_OFF 0
+#define SELFGPU_CLOSURE_INDICATOR 1
+#define SELFGPU_CLOSURE_MLP 2
+#define SELFGPU_MLP_WEIGHTS 2208 /* bf16: W1 (32 x 36, row-major), W2 (32 x 32), w3 (32) */
+#define SELFGPU_MLP_PARAMS 137   /* float: b1 (32), b2 (32), b3, feature minima (36), maxima (36) */
+int selfgpu_model2d_set_closure(selfgpu_model2d* m, int mode, double c, double s0, double kappa,
+                                const double* controlPoints);
+
+/* Closure MLP 36 -> 32 -> 32 -> 1 (ReLU, output clamped to [0, 1]): bfloat16
+ * weights (raw 16-bit patterns) and float biases / feature ranges, host arrays. */
+int selfgpu_model2d_set_mlp(selfgpu_model2d* m, const uint16_t* weights, const float* params);
+
+/* Copies (on the engine's stream) the last stage's element viscosity (nEl
+ * doubles), the activation applied and the indicator's activation (nEl floats
+ * each; the latter written in mode 2) into caller-owned device arrays (each
+ * may be NULL), and returns on the host the number of MLP fallbacks since the
+ * last reset. */
+int selfgpu_model2d_closure_state(selfgpu_model2d* m, double* nu, float* activation, float* indicatorActivation,
+                                  int* fallbacks, int resetFallbacks);
+
+/* Modal transform T(k,i) = w_i sqrt((2k+1)/2) L_k(x_i) (P x P, k fastest). */
+int selfgpu_modal_matrix(int N, const double* controlPoints, const double* qWeights, double* T);
+
+/* Training-data harvest: per element of a device CIG state (P,P,4,nEl), the
+ * indicator activation of the density and the 36 closure features (36, nEl),
+ * float32 device outputs (either may be NULL; features need N >= 5). */
+int selfgpu_cig2d_closure_features(const double* solution, int N, int nEl, const double* controlPoints,
+                                   const double* qWeights, double s0, double kappa, float* activation,
+                                   float* features, void* stream);
+
+/* Training of the closure MLP on device samples features (36, n) and labels
+ * (n): minibatch Adam on float32 master weights with the forward pass on
+ * bfloat16-rounded weights (quantisation-aware), squared error on the
+ * clamped output.  params (host, in/out) holds the float32 masters in the
+ * order W1 (32x36), b1 (32), W2 (32x32), b2 (32), w3 (32), b3 (1): 2273
+ * floats.  lossPerEpoch (host, epochs floats) may be NULL. */
+#define SELFGPU_MLP_MASTER 2273
+int selfgpu_mlp_train(const float* features, const float* labels, int n, int epochs, int batch, float lr,
+                      unsigned long long seed, float* params, float* lossPerEpoch, void* stream);
+
+/* Inference of the closure MLP over n device feature vectors (36, n) into
+ * out (n floats), with the device-side weights layout of set_mlp (host arrays). */
+int selfgpu_mlp_infer(const float* features, int n, const uint16_t* weights, const float* params, float* out,
+                      void* stream);
 
 #ifdef __cplusplus
 }

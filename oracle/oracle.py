@@ -37,7 +37,7 @@ def lib(fast: bool = False):
         L.orc_model_field_size.restype = ctypes.c_longlong
         for fn in ("orc_model_free", "orc_model_tendency", "orc_model_rk3", "orc_model_set",
                    "orc_model_get", "orc_model_set_params", "orc_model_entropy",
-                   "orc_model_arcmin", "orc_model_field_size"):
+                   "orc_model_arcmin", "orc_model_field_size", "orc_model_set_closure"):
             getattr(L, fn).argtypes = None
         _libs[name] = L
     return _libs[name]
@@ -267,6 +267,58 @@ class Model:
 
     def arcmin(self):
         return self.L.orc_model_arcmin(self.h)
+
+    def set_closure(self, mode, c=1.0, s0=None, kappa=1.0):
+        """Artificial-viscosity closure (CIG): 0 off, 1 modal-decay indicator,
+        2 element viscosity given through set("avNu", ...)."""
+        if s0 is None:
+            s0 = default_s0(self.N)
+        rc = self.L.orc_model_set_closure(self.h, int(mode), ctypes.c_double(c), ctypes.c_double(s0),
+                                          ctypes.c_double(kappa))
+        if rc != 0:
+            raise ValueError("closure needs a CompressibleIdealGas2D model")
+
+
+def default_s0(N):
+    """Indicator threshold s0 = log10(1/N^4) (Persson & Peraire)."""
+    return float(-4.0 * np.log10(N))
+
+
+def modal_matrix(N, quad=GAUSS):
+    T = _z(N + 1, N + 1)
+    lib().orc_modal_matrix(N, quad, _p(T))
+    return T
+
+
+def closure_features(q, N, s0=None, kappa=1.0, quad=GAUSS):
+    """Modal-decay activation of the density (nEl,) and the 36 closure
+    features (36, nEl) of a (P,P,4,nEl) CompressibleIdealGas2D state."""
+    q = np.asfortranarray(q, dtype=np.float64)
+    nEl = q.shape[3]
+    T = modal_matrix(N, quad)
+    act, feat = np.zeros(nEl), _z(36, nEl)
+    if s0 is None:
+        s0 = default_s0(N)
+    lib().orc_closure_features(_p(T), _p(q), int(N), int(nEl), ctypes.c_double(s0), ctypes.c_double(kappa),
+                               _p(act), _p(feat))
+    return act, feat
+
+
+def bf16_round(x):
+    """Round float32 values to bfloat16 (nearest, ties to even), returned as float32."""
+    b = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) >> 16
+    return (b.astype(np.uint32) << 16).view(np.float32).reshape(np.shape(x))
+
+
+def mlp_forward(feat, W1, b1, W2, b2, w3, b3):
+    """Closure MLP 36 -> 32 -> 32 -> 1 with bfloat16 weights and float32
+    accumulation; output clamp(z, 0, 1).  feat is (36, n); returns (n,)."""
+    f = np.asarray(feat, dtype=np.float32)
+    h1 = np.maximum(bf16_round(W1) @ f + np.asarray(b1, np.float32)[:, None], 0)
+    h2 = np.maximum(bf16_round(W2) @ h1 + np.asarray(b2, np.float32)[:, None], 0)
+    z = bf16_round(np.asarray(w3, np.float32)) @ h2 + np.float32(b3)
+    return np.clip(z, 0.0, 1.0)
 
 
 def set_threads(n, fast=False):

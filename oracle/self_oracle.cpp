@@ -52,6 +52,8 @@ static const double TOL = DBL_EPSILON;           // src/SELF_Constants.f90:42
 
 using Vec = std::vector<double>;
 
+static const int kOrcMaxP = 16;
+
 // ---------------------------------------------------------------- quadrature
 // src/SELF_Quadrature.f90:342-383 (Kopriva Alg. 22)
 static void LegendrePolynomial(int N, double x, double& l, double& dl) {
@@ -658,6 +660,95 @@ static void Determinant2D(const double* t, double* det, int N, int nVar, int nEl
                                 t[TE(0, 1, i, j, v, e)] * t[TE(1, 0, i, j, v, e)];
 }
 
+// ------------------------------------------------- artificial-viscosity closure
+// Not part of the reference: the shock closure the CompressibleIdealGas2D
+// tendency gains for discontinuous data.  The pieces it is built from are the
+// reference's own operators: BassiRebaySides + GradientBR (src/SELF_MappedData.f90:
+// 919-1078), VectorBoundaryInterp (src/SELF_Lagrange.f90:2284-2316),
+// SideExchange (src/SELF_MappedData.f90:1870-1958) and the diffusive flux
+// templates of Advection2D (src/models/hip/SELF_Advection2D.cpp:66-95, :140-175),
+// generalised from one diffusivity to one viscosity per element.  Physical
+// sides carry no viscous flux (no diffusion through walls or open boundaries).
+//
+// Modal decay indicator: Persson & Peraire, "Sub-cell shock capturing for
+// discontinuous Galerkin methods", AIAA 2006-112.  With orthonormal Legendre
+// modes c_kl of the density, S = sum_{max(k,l)=N} c_kl^2 / sum c_kl^2,
+// s = log10 S and the activation a(s) = 0 below s0 - kappa, 1 above
+// s0 + kappa, (1 + sin(pi (s - s0) / (2 kappa))) / 2 between.  The element
+// viscosity is nu = a * c_av * h / N * lambda, lambda = max over nodes of
+// |u| + c and h = sqrt(element area).
+
+// T(k,i) = w_i Lt_k(x_i), Lt_k = sqrt((2k+1)/2) L_k: c = T q T^T for nodal q on
+// Gauss nodes (exact: the products have degree <= 2N).
+static void ModalMatrix(int N, const double* x, const double* w, double* T) {
+  int P = N + 1;
+  for (int i = 0; i < P; ++i)
+    for (int k = 0; k < P; ++k) {
+      double l, dl;
+      LegendrePolynomial(k, x[i], l, dl);
+      T[k + P * i] = (std::sqrt((2.0 * k + 1.0) / 2.0) * l) * w[i];
+    }
+}
+
+// c[k + P l] = sum_j T(l,j) sum_i T(k,i) q(i,j); q is one element's (P,P) block.
+static void ModalCoefficients(const double* T, const double* q, double* c, int P) {
+  double t[kOrcMaxP * kOrcMaxP];
+  for (int j = 0; j < P; ++j)
+    for (int k = 0; k < P; ++k) {
+      double acc = 0.0;
+      for (int i = 0; i < P; ++i) acc = acc + T[k + P * i] * q[i + P * j];
+      t[k + P * j] = acc;
+    }
+  for (int l = 0; l < P; ++l)
+    for (int k = 0; k < P; ++k) {
+      double acc = 0.0;
+      for (int j = 0; j < P; ++j) acc = acc + T[l + P * j] * t[k + P * j];
+      c[k + P * l] = acc;
+    }
+}
+
+static double ModalDecayActivation(const double* c, int P, double s0, double kappa) {
+  int N = P - 1;
+  double top = 0.0, total = 0.0;
+  for (int l = 0; l < P; ++l)
+    for (int k = 0; k < P; ++k) {
+      double e = c[k + P * l] * c[k + P * l];
+      total = total + e;
+      if (k == N || l == N) top = top + e;
+    }
+  if (!(top > 0.0) || !(total > 0.0)) return 0.0;
+  double sv = std::log10(top / total);
+  if (sv < s0 - kappa) return 0.0;
+  if (sv > s0 + kappa) return 1.0;
+  return 0.5 * (1.0 + std::sin(PI * (sv - s0) / (2.0 * kappa)));
+}
+
+// 18 features of one variable's modes: the energy fractions of the six highest
+// shells max(k,l) = m, of the six highest xi-degrees k and of the six highest
+// eta-degrees l (m, k, l = N-5..N), each mapped to (log10(max(E/Et, 1e-16)) + 8) / 8.
+static void ModalFeatures(const double* c, int P, double* f) {
+  int N = P - 1;
+  double total = 0.0, sh[kOrcMaxP] = {0}, ex[kOrcMaxP] = {0}, ey[kOrcMaxP] = {0};
+  for (int l = 0; l < P; ++l)
+    for (int k = 0; k < P; ++k) {
+      double e = c[k + P * l] * c[k + P * l];
+      total = total + e;
+      int m = k > l ? k : l;
+      sh[m] = sh[m] + e;
+      ex[k] = ex[k] + e;
+      ey[l] = ey[l] + e;
+    }
+  for (int r = 0; r < 6; ++r) {
+    int m = N - 5 + r;
+    double fr[3] = {sh[m], ex[m], ey[m]};
+    for (int g = 0; g < 3; ++g) {
+      double q = total > 0.0 ? fr[g] / total : 0.0;
+      if (q < 1e-16) q = 1e-16;
+      f[r + 6 * g] = (std::log10(q) + 8.0) / 8.0;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------- mesh
 // Structured quadrilateral generator (the reference reads 2-D meshes only from
 // HOPr HDF5 files, src/SELF_Mesh.f90:852-1016; hazard H10).  Conventions follow
@@ -892,6 +983,10 @@ struct Model {
   // CIG
   Field prim, diag, prescSol, prescPrim, prescDiag, env;
   Vec envGrad;
+  // artificial-viscosity closure (CIG): 0 off, 1 modal-decay indicator, 2 element viscosity given
+  int closure = 0;
+  double avC = 1.0, avS0 = 0.0, avKappa = 1.0;
+  Vec modalT, avNu, avAct, avH, avAvg, avGrad, avGB, avGExt;
 
   size_t nIn(int nv) const { return (size_t)P * P * nv * nEl; }
   size_t nB(int nv) const { return (size_t)P * nv * 4 * nEl; }
@@ -1232,6 +1327,89 @@ struct Model {
         }
   }
 
+  // --- artificial-viscosity closure (see the closure helpers above)
+  void closureEnable(int mode, double c, double s0, double kappa) {
+    closure = mode;
+    avC = c;
+    avS0 = s0;
+    avKappa = kappa;
+    modalT.assign((size_t)P * P, 0.0);
+    ModalMatrix(N, interp.ctrl.data(), interp.qw.data(), modalT.data());
+    if (avNu.size() != (size_t)nEl) avNu.assign(nEl, 0.0);
+    avAct.assign(nEl, 0.0);
+    avH.assign(nEl, 0.0);
+    for (int e = 0; e < nEl; ++e) {  // h = sqrt(sum_ij w_i w_j J_ij)
+      double area = 0.0;
+      for (int j = 0; j < P; ++j)
+        for (int i = 0; i < P; ++i) area = area + interp.qw[i] * interp.qw[j] * geo->J[i + P * (j + P * (size_t)e)];
+      avH[e] = std::sqrt(area);
+    }
+    avAvg.assign(nB(4), 0.0);
+    avGrad.assign(2 * nIn(4), 0.0);
+    avGB.assign(2 * nB(4), 0.0);
+    avGExt.assign(2 * nB(4), 0.0);
+  }
+  // element viscosity from the modal-decay indicator of the density (closure 1)
+  void cigClosureViscosity() {
+    int nVar = 4;
+    OMP_FOR
+    for (int e = 0; e < nEl; ++e) {
+      double c[kOrcMaxP * kOrcMaxP];
+      ModalCoefficients(modalT.data(), &sol.in[SC(0, 0, 2, e)], c, P);
+      double a = ModalDecayActivation(c, P, avS0, avKappa);
+      double lam = 0.0;
+      for (int j = 0; j < P; ++j)
+        for (int i = 0; i < P; ++i) {
+          double u = prim.in[SC(i, j, 0, e)], v = prim.in[SC(i, j, 1, e)];
+          double w = std::sqrt(u * u + v * v) + diag.in[SC(i, j, 2, e)];
+          if (w > lam) lam = w;
+        }
+      avAct[e] = a;
+      avNu[e] = a * avC * avH[e] / (double)N * lam;
+    }
+  }
+  // BR1 gradient of the conservative variables and the viscous traces nu grad q
+  void cigClosureGradient() {
+    int nVar = 4;
+    BassiRebaySides(avAvg.data(), sol.b.data(), sol.ext.data(), N, 4, nEl);
+    GradientBR(sol.in.data(), avAvg.data(), geo->dsdx.data(), geo->J.data(), geo->nHat.data(), geo->nScale.data(),
+               avGrad.data(), interp.dgM.data(), interp.bM.data(), interp.qw.data(), N, 4, nEl);
+    OMP_FOR
+    for (int e = 0; e < nEl; ++e)
+      for (size_t k = 0; k < 2 * (size_t)P * P * 4; ++k) avGrad[k + 2 * (size_t)P * P * 4 * e] *= avNu[e];
+    VectorBoundaryInterp2D(interp.bM.data(), avGrad.data(), avGB.data(), N, 4, nEl);
+    SideExchangeVector(avGExt.data(), avGB.data(), sideInfo.data(), N, 4, nEl);
+  }
+  // viscous contributions on the contravariant volume flux and on the face flux
+  void cigClosureFluxes() {
+    int nVar = 4;
+    OMP_FOR
+    for (int e = 0; e < nEl; ++e)
+      for (int v = 0; v < 4; ++v)
+        for (int j = 0; j < P; ++j)
+          for (int i = 0; i < P; ++i) {
+            size_t a = 4 * (i + P * (j + P * (size_t)e));
+            double gx = avGrad[VE(0, i, j, v, e)], gy = avGrad[VE(1, i, j, v, e)];
+            double f1 = -(geo->dsdx[a + 0] * gx + geo->dsdx[a + 1] * gy);
+            double f2 = -(geo->dsdx[a + 2] * gx + geo->dsdx[a + 3] * gy);
+            flux[VE(0, i, j, v, e)] = flux[VE(0, i, j, v, e)] + f1;
+            flux[VE(1, i, j, v, e)] = flux[VE(1, i, j, v, e)] + f2;
+          }
+    OMP_FOR
+    for (int e = 0; e < nEl; ++e)
+      for (int s = 0; s < 4; ++s) {
+        if (sideInfo[5 * (s + 4 * (size_t)e) + 4] != 0) continue;  // no viscous flux through physical sides
+        for (int v = 0; v < 4; ++v)
+          for (int i = 0; i < P; ++i) {
+            size_t b = i + P * (s + 4 * (size_t)e);
+            double n1 = geo->nHat[2 * b], n2 = geo->nHat[2 * b + 1], nmag = geo->nScale[b];
+            double in = avGB[VEB(0, i, v, s, e)] * n1 + avGB[VEB(1, i, v, s, e)] * n2;
+            double ex = avGExt[VEB(0, i, v, s, e)] * n1 + avGExt[VEB(1, i, v, s, e)] * n2;
+            fluxBN[SCB(i, v, s, e)] = fluxBN[SCB(i, v, s, e)] + -0.5 * (in + ex) * nmag;
+          }
+      }
+  }
+
   // src/SELF_Model2D.f90:816-859
   void CalculateTendency() {
     if (kind == SW) swPreTendency();
@@ -1241,7 +1419,12 @@ struct Model {
     if (kind == LSW) { lswBC(); lswSource(); lswRiemann(); lswFlux(); }
     if (kind == SW) { swBC(); swSource(); swRiemann(); swFlux(); }
     if (kind == CIG) { cigBC(); cigSource(); cigLLF(); cigFlux(); }
+    if (kind == CIG && closure != 0) {
+      if (closure == 1) cigClosureViscosity();
+      cigClosureGradient();
+    }
     ContravariantProjection(flux.data(), geo->dsdx.data(), N, nVar, nEl);
+    if (kind == CIG && closure != 0) cigClosureFluxes();
     VectorDGDivergence2D(interp.dgM.data(), interp.bM.data(), interp.qw.data(), flux.data(),
                          fluxBN.data(), fdiv.in.data(), N, nVar, nEl);
     JacobianWeightScalar(fdiv.in.data(), geo->J.data(), N, nVar, nEl);
@@ -1478,6 +1661,11 @@ static Vec* field_ptr(Model& m, const std::string& n) {
   if (n == "environmentals") return &m.env.in;
   if (n == "environmentalsGradient") return &m.envGrad;
   if (n == "prescribedSolution.boundary") return &m.prescSol.b;
+  if (n == "avNu") return m.avNu.empty() ? nullptr : &m.avNu;
+  if (n == "avActivation") return m.avAct.empty() ? nullptr : &m.avAct;
+  if (n == "avH") return m.avH.empty() ? nullptr : &m.avH;
+  if (n == "avGradient") return m.avGrad.empty() ? nullptr : &m.avGrad;
+  if (n == "avGradient.boundary") return m.avGB.empty() ? nullptr : &m.avGB;
   return nullptr;
 }
 
@@ -1559,6 +1747,38 @@ int orc_model_get(void* p, const char* name, double* out) {
   if (!f) return -1;
   std::memcpy(out, f->data(), sizeof(double) * f->size());
   return 0;
+}
+
+// closure 0 off, 1 modal-decay indicator, 2 element viscosity set through "avNu"
+int orc_model_set_closure(void* p, int closure, double c, double s0, double kappa) {
+  Model& m = ((OrcModel*)p)->m;
+  if (m.kind != CIG || closure < 0 || closure > 2) return -1;
+  m.closureEnable(closure, c, s0, kappa);
+  return 0;
+}
+
+void orc_modal_matrix(int N, int quad, double* T) {
+  Lagrange L;
+  L.init(N, quad, N, UNIFORM);
+  ModalMatrix(N, L.ctrl.data(), L.qw.data(), T);
+}
+
+// Per element of a (P,P,4,nEl) CIG state: modal-decay activation of the density
+// and the 36 closure features (density, then total energy) in feat(36, nEl).
+void orc_closure_features(const double* T, const double* q, int N, int nEl, double s0, double kappa, double* act,
+                          double* feat) {
+  int P = N + 1;
+  OMP_FOR
+  for (int e = 0; e < nEl; ++e) {
+    double c[kOrcMaxP * kOrcMaxP];
+    ModalCoefficients(T, q + (size_t)P * P * (2 + 4 * (size_t)e), c, P);
+    if (act) act[e] = ModalDecayActivation(c, P, s0, kappa);
+    if (feat) {
+      ModalFeatures(c, P, feat + 36 * (size_t)e);
+      ModalCoefficients(T, q + (size_t)P * P * (3 + 4 * (size_t)e), c, P);
+      ModalFeatures(c, P, feat + 36 * (size_t)e + 18);
+    }
+  }
 }
 
 void orc_model_tendency(void* p) { ((OrcModel*)p)->m.CalculateTendency(); }

@@ -40,6 +40,14 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
+CLOSURE_OFF, CLOSURE_INDICATOR, CLOSURE_MLP = 0, 1, 2
+
+
+def default_s0(N):
+    """Modal-decay threshold s0 = log10(1 / N^4) (Persson & Peraire)."""
+    return float(-4.0 * np.log10(N))
+
+
 class Lagrange:
     """Lagrange%Init (src/SELF_Lagrange.f90:521-615), built on the host."""
 
@@ -350,6 +358,34 @@ class CompressibleIdealGas2D(Model2D):
         self._set_field("prescribedSolution.boundary", self._bnd_interp(self.solution, 4))
         self._set_field("prescribedPrimitive.boundary", self._bnd_interp(prim, 4))
         self._set_field("prescribedDiagnostics.boundary", self._bnd_interp(diag, 4))
+
+    # ---- shock closure (artificial viscosity through BR1)
+    def SetClosure(self, mode, c=1.0, s0=None, kappa=1.0, mlp=None):
+        """mode CLOSURE_OFF / CLOSURE_INDICATOR / CLOSURE_MLP; nu_e = a c h_e / N max(|u| + c_sound),
+        a from the modal-decay indicator (threshold s0 = log10(N^-4) by default, half-width kappa)
+        or from the closure MLP (a ClosureMLP, N >= 5)."""
+        if mlp is not None:
+            w, prm = mlp.device_weights(), mlp.device_params()
+            check(lib().selfgpu_model2d_set_mlp(self._h, w.ctypes.data_as(ctypes.c_void_p),
+                                                prm.ctypes.data_as(ctypes.c_void_p)))
+        if s0 is None:
+            s0 = default_s0(self.N)
+        self.closure = (mode, c, s0, kappa)
+        check(lib().selfgpu_model2d_set_closure(self._h, int(mode), float(c), float(s0), float(kappa),
+                                                self.interp.controlPoints.ctypes.data_as(ctypes.c_void_p)))
+
+    def ClosureState(self, reset=False):
+        """(nu (nEl,) f64, activation (nEl,) f32, indicator activation (nEl,) f32, MLP fallbacks)
+        of the last tendency / RK stage."""
+        nEl = self.nElem
+        nu = torch.empty(nEl, device="cuda", dtype=torch.float64)
+        act = torch.empty(nEl, device="cuda", dtype=torch.float32)
+        ind = torch.empty(nEl, device="cuda", dtype=torch.float32)
+        fb = ctypes.c_int(0)
+        torch.cuda.synchronize()
+        check(lib().selfgpu_model2d_closure_state(self._h, nu.data_ptr(), act.data_ptr(), ind.data_ptr(),
+                                                  ctypes.byref(fb), int(reset)))
+        return nu, act, ind, fb.value
 
     def CalculateEntropy(self):
         prim = self._pointwise("primitive")

@@ -1,0 +1,441 @@
+// Artificial-viscosity closure of the CompressibleIdealGas2D tendency.
+//
+// Not a reference routine: the shock closure built from the reference's own
+// operators -- BassiRebaySides + GradientBR (src/SELF_MappedData.f90:919-1078),
+// VectorBoundaryInterp (src/SELF_Lagrange.f90:2284-2316), SideExchange of a
+// vector (src/SELF_MappedData.f90:1870-1958) and the Advection2D diffusive flux
+// templates (src/models/hip/SELF_Advection2D.cpp:66-95, :140-175) -- with one
+// viscosity per element instead of one diffusivity.
+//
+// With the closure on, each RK stage is two launches:
+//   k_av_prep   per element: element viscosity nu (modal-decay indicator of the
+//               density, or the closure MLP with the indicator as fallback),
+//               the BR1 gradient of the four conservative variables from the
+//               averaged traces of the stage's trace cache, the contravariant
+//               viscous volume flux -(dsdx^T nu grad q) and the face traces of
+//               nu grad q;
+//   the stage   kernel adds the viscous volume flux to its contravariant flux
+//               and, on exchanged sides, -1/2 (nu grad q_in + nu grad q_ex) . n
+//               nScale to its face flux, the exterior value coming from the
+//               neighbour's traces; physical sides carry no viscous flux.
+//
+// Modal decay indicator (Persson & Peraire, AIAA 2006-112): c_kl are the
+// orthonormal Legendre modes of the density, S = sum_{max(k,l)=N} c^2 /
+// sum c^2, s = log10 S, activation a = 0 below s0 - kappa, 1 above s0 + kappa,
+// (1 + sin(pi (s - s0) / (2 kappa))) / 2 between; nu = a c_av h / N lambda with
+// lambda = max over nodes of |u| + c and h = sqrt(element area).
+//
+// Closure MLP: 36 features (per variable, density then total energy, the
+// energy fractions of the six highest shells max(k,l), xi-degrees and
+// eta-degrees, log-scaled) -> 32 -> 32 -> 1, ReLU, bfloat16 weights, float32
+// accumulation, output clamp(z, 0, 1) replaces a.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "fused_stage.cuh"
+
+namespace selfgpu {
+
+constexpr int kMlpIn = 36, kMlpHidden = 32;
+constexpr int kMlpWeights = kMlpHidden * kMlpIn + kMlpHidden * kMlpHidden + kMlpHidden;  // bf16 values
+constexpr int kMlpFloats = kMlpHidden + kMlpHidden + 1 + 2 * kMlpIn;                    // b1 b2 b3 fmin fmax
+constexpr double kAvPi = 3.141592653589793;                                             // 4 atan(1)
+constexpr float kMlpRangeMargin = 0.05f;
+
+enum AvMode { AV_OFF = 0, AV_INDICATOR = 1, AV_MLP = 2 };
+
+struct AvArgs {
+  int nEl;
+  int mode;  // AV_INDICATOR or AV_MLP
+  const double* q;
+  const double* dsdx;
+  const double* J;
+  const double* nHat;
+  const double* nScale;
+  const int* sideInfo;
+  const void* trIn;     // trace cache of this stage (bulk type); conservative traces are fields 0..3
+  const double* presc;  // prescribed solution boundary (P,4,4,nEl) or null
+  const double* hEl;    // element size sqrt(area), (nEl)
+  double gamma, avC, s0, kappa;
+  double* nu;          // element viscosity (nEl)
+  float* act;          // activation applied (nEl)
+  float* actInd;       // indicator activation (nEl), written in AV_MLP mode
+  int* fallbacks;      // AV_MLP: elements whose features left the training range
+  void* visc;          // contravariant viscous volume flux (P*P, 2, 4, nEl), bulk type
+  void* vtr;           // per (element, side): nu grad q traces at [i + P (d + 2 v)], bulk type
+  const __nv_bfloat16* mlpW;  // W1 (32 x 36, row-major), W2 (32 x 32), w3 (32)
+  const float* mlpB;          // b1 (32), b2 (32), b3, fmin (36), fmax (36)
+  double T[kMaxP * kMaxP];    // modal matrix T(k,i) = w_i Lt_k(x_i) at [k + P i]
+  double dgM[kMaxP * kMaxP];
+  double bM[2 * kMaxP];
+  double qw[kMaxP];
+};
+
+template <typename R>
+__device__ __forceinline__ R av_log10(R x) {
+  if constexpr (sizeof(R) == 8) return log10(x);
+  else return log10f(x);
+}
+template <typename R>
+__device__ __forceinline__ R av_sin(R x) {
+  if constexpr (sizeof(R) == 8) return sin(x);
+  else return sinf(x);
+}
+template <typename R>
+__device__ __forceinline__ R av_sqrt(R x) {
+  if constexpr (sizeof(R) == 8) return sqrt(x);
+  else return sqrtf(x);
+}
+
+// Modal decay activation from one variable's modes c[k + P l] (one thread).
+template <int P, typename R>
+__device__ R modal_activation(const R* c, double s0, double kappa) {
+  constexpr int N = P - 1;
+  R top = (R)0, total = (R)0;
+  for (int l = 0; l < P; ++l)
+    for (int k = 0; k < P; ++k) {
+      const R e = c[k + P * l] * c[k + P * l];
+      total = total + e;
+      if (k == N || l == N) top = top + e;
+    }
+  if (!(top > (R)0) || !(total > (R)0)) return (R)0;
+  const R sv = av_log10<R>(top / total);
+  if (sv < (R)s0 - (R)kappa) return (R)0;
+  if (sv > (R)s0 + (R)kappa) return (R)1;
+  return (R)0.5 * ((R)1 + av_sin<R>((R)kAvPi * (sv - (R)s0) / ((R)2 * (R)kappa)));
+}
+
+// The 18 features of one variable's modes (one thread); requires P >= 6.
+template <int P, typename R>
+__device__ void modal_features(const R* c, float* f) {
+  constexpr int N = P - 1;
+  R total = (R)0, sh[P], ex[P], ey[P];
+#pragma unroll
+  for (int k = 0; k < P; ++k) sh[k] = ex[k] = ey[k] = (R)0;
+  for (int l = 0; l < P; ++l)
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+      const R e = c[k + P * l] * c[k + P * l];
+      total = total + e;
+      const int m = k > l ? k : l;
+      sh[m] = sh[m] + e;
+      ex[k] = ex[k] + e;
+      ey[l] = ey[l] + e;
+    }
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    const int m = N - 5 + r;
+    const R fr[3] = {sh[m], ex[m], ey[m]};
+#pragma unroll
+    for (int g = 0; g < 3; ++g) {
+      R q = total > (R)0 ? fr[g] / total : (R)0;
+      if (q < (R)1e-16) q = (R)1e-16;
+      f[r + 6 * g] = (float)((av_log10<R>(q) + (R)8) / (R)8);
+    }
+  }
+}
+
+// ------------------------------------------------------------ prep kernel
+template <int P, typename R>
+struct AvSmem {
+  static constexpr int PP = P * P;
+  R q[4][PP];
+  R dsdx[4][PP];  // (dsdx11, dsdx21, dsdx12, dsdx22) per node
+  R avg[4][4][P];
+  R g[2][4][PP];  // nu grad q
+  R tt[2][PP];
+  R c[2][PP];
+  R lam[PP];
+  float feat[kMlpIn];
+  float h1[kMlpHidden];
+  float h2[kMlpHidden];
+  R nu;
+};
+
+template <int P, typename R>
+constexpr int av_elems_per_block() {
+  int e = 128 / (P * P);
+  if (e < 1) e = 1;
+  while (e > 1 && (size_t)e * sizeof(AvSmem<P, R>) > 30 * 1024) --e;
+  return e;
+}
+
+template <int P, typename R, int EPB>
+__global__ void __launch_bounds__(EPB* P* P) k_av_prep(const AvArgs a) {
+  constexpr int PP = P * P, N = P - 1, VS = visc_side_stride<P>();
+  constexpr int TS = trace_side_stride<P, 9, R>();
+  __shared__ AvSmem<P, R> sm_all[EPB];
+  __shared__ double sT[PP], sdg[PP], sb[2 * P], sw[P];
+  __shared__ float sW1[kMlpHidden * kMlpIn], sW2[kMlpHidden * kMlpHidden], sw3[kMlpHidden], sB[kMlpFloats];
+
+  const int tid = threadIdx.x;
+  const int slot = tid / PP;
+  const int t = tid - slot * PP;
+  const int i = t % P, j = t / P;
+  AvSmem<P, R>& sm = sm_all[slot];
+  const bool mlp = (a.mode == AV_MLP) && (P >= 6);
+
+  for (int k = tid; k < PP; k += blockDim.x) {
+    sT[k] = a.T[k];
+    sdg[k] = a.dgM[k];
+  }
+  for (int k = tid; k < 2 * P; k += blockDim.x) sb[k] = a.bM[k];
+  for (int k = tid; k < P; k += blockDim.x) sw[k] = a.qw[k];
+  if (mlp) {
+    for (int k = tid; k < kMlpHidden * kMlpIn; k += blockDim.x) sW1[k] = __bfloat162float(a.mlpW[k]);
+    for (int k = tid; k < kMlpHidden * kMlpHidden; k += blockDim.x)
+      sW2[k] = __bfloat162float(a.mlpW[kMlpHidden * kMlpIn + k]);
+    for (int k = tid; k < kMlpHidden; k += blockDim.x)
+      sw3[k] = __bfloat162float(a.mlpW[kMlpHidden * kMlpIn + kMlpHidden * kMlpHidden + k]);
+    for (int k = tid; k < kMlpFloats; k += blockDim.x) sB[k] = a.mlpB[k];
+  }
+
+  const long long e = (long long)blockIdx.x * EPB + slot;
+  const bool live = e < a.nEl;
+  const R* trIn = reinterpret_cast<const R*>(a.trIn);
+  const R gam = (R)a.gamma;
+
+  if (live) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) sm.q[v][t] = (R)a.q[t + (long long)PP * (v + 4 * e)];
+    const double* gd = a.dsdx + 4 * (t + (long long)PP * e);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) sm.dsdx[k][t] = (R)gd[k];
+    // wave speed |u| + c at this node (src/models/SELF_CompressibleIdealGas2D.f90:1090-1110)
+    const R rho = sm.q[2][t], u = sm.q[0][t] / rho, v = sm.q[1][t] / rho;
+    const R ke = (R)0.5 * (sm.q[0][t] * u + sm.q[1][t] * v);
+    const R p = (gam - (R)1) * (sm.q[3][t] - ke);
+    const R c = av_sqrt<R>(gam * p / rho);
+    sm.lam[t] = av_sqrt<R>(u * u + v * v) + c;
+    // averaged conservative traces (BassiRebaySides) with the stage's exterior states
+    for (int k = t; k < 4 * P; k += PP) {
+      const int s1 = k / P, ii = k % P;
+      const int* si = a.sideInfo + 5 * (s1 + 4 * e);
+      const R* own = trIn + (long long)TS * (s1 + 4 * e);
+      R L[4], X[4];
+#pragma unroll
+      for (int w = 0; w < 4; ++w) {
+        L[w] = own[ii + P * w];
+        X[w] = (R)0;
+      }
+      const int bcid = si[4];
+      if (bcid == 0) {
+        const long long e2 = si[2] - 1;
+        const int s2 = si[3] / 10 - 1, flip = si[3] % 10;
+        const R* nb = trIn + (long long)TS * (s2 + 4 * e2);
+        const int i2 = flip ? N - ii : ii;
+#pragma unroll
+        for (int w = 0; w < 4; ++w) X[w] = nb[i2 + P * w];
+      } else if (si[2] == 0) {  // physical side: the boundary condition's exterior state
+        if (bcid == SG_BC_NONORMALFLOW) {
+          const double2 nh = reinterpret_cast<const double2*>(a.nHat)[ii + (long long)P * (s1 + 4 * e)];
+          reflect<R>(L[0], L[1], nh.x, nh.y, X[0], X[1]);
+          X[2] = L[2];
+          X[3] = L[3];
+        } else if ((bcid == SG_BC_PRESCRIBED || bcid == SG_BC_RADIATION) && a.presc) {
+#pragma unroll
+          for (int w = 0; w < 4; ++w) X[w] = (R)a.presc[ii + (long long)P * (w + 4 * (s1 + 4 * e))];
+        }
+      }
+#pragma unroll
+      for (int w = 0; w < 4; ++w) sm.avg[s1][w][ii] = (R)0.5 * (L[w] + X[w]);
+    }
+  }
+  __syncthreads();
+  // modal transform, pass 1: tt(k, j) = sum_i T(k,i) q(i,j) (density, and total energy for the MLP)
+  if (live) {
+    const int k = i, jj = j;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      if (r == 1 && !mlp) break;
+      const R* qv = sm.q[2 + r];
+      R acc = (R)0;
+#pragma unroll
+      for (int m = 0; m < P; ++m) acc = acc + (R)sT[k + P * m] * qv[m + P * jj];
+      sm.tt[r][k + P * jj] = acc;
+    }
+  }
+  __syncthreads();
+  // pass 2: c(k, l) = sum_j T(l,j) tt(k,j)
+  if (live) {
+    const int k = i, l = j;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      if (r == 1 && !mlp) break;
+      R acc = (R)0;
+#pragma unroll
+      for (int m = 0; m < P; ++m) acc = acc + (R)sT[l + P * m] * sm.tt[r][k + P * m];
+      sm.c[r][k + P * l] = acc;
+    }
+  }
+  __syncthreads();
+  R actInd = (R)0;
+  if (live && t == 0) actInd = modal_activation<P, R>(sm.c[0], a.s0, a.kappa);
+  if (mlp) {
+    if (live && t < 2) {
+      if constexpr (P >= 6) modal_features<P, R>(sm.c[t], sm.feat + 18 * t);
+    }
+    __syncthreads();
+    if (live && t < kMlpHidden) {
+      float acc = 0.f;
+#pragma unroll 4
+      for (int k = 0; k < kMlpIn; ++k) acc = fmaf(sW1[t * kMlpIn + k], sm.feat[k], acc);
+      acc = acc + sB[t];
+      sm.h1[t] = acc > 0.f ? acc : 0.f;
+    }
+    __syncthreads();
+    if (live && t < kMlpHidden) {
+      float acc = 0.f;
+#pragma unroll 4
+      for (int k = 0; k < kMlpHidden; ++k) acc = fmaf(sW2[t * kMlpHidden + k], sm.h1[k], acc);
+      acc = acc + sB[kMlpHidden + t];
+      sm.h2[t] = acc > 0.f ? acc : 0.f;
+    }
+    __syncthreads();
+  }
+  if (live && t == 0) {
+    R act = actInd;
+    if (mlp) {
+      bool inRange = true;
+      const float* fmin = sB + 2 * kMlpHidden + 1;
+      const float* fmax = fmin + kMlpIn;
+      for (int k = 0; k < kMlpIn; ++k)
+        inRange = inRange && sm.feat[k] >= fmin[k] - kMlpRangeMargin && sm.feat[k] <= fmax[k] + kMlpRangeMargin;
+      if (inRange) {
+        float z = 0.f;
+        for (int k = 0; k < kMlpHidden; ++k) z = fmaf(sw3[k], sm.h2[k], z);
+        z = z + sB[2 * kMlpHidden];
+        act = (R)(z < 0.f ? 0.f : (z > 1.f ? 1.f : z));
+      } else if (a.fallbacks) {
+        atomicAdd(a.fallbacks, 1);
+      }
+      if (a.actInd) a.actInd[e] = (float)actInd;
+    }
+    R lam = (R)0;
+    for (int k = 0; k < PP; ++k)
+      if (sm.lam[k] > lam) lam = sm.lam[k];
+    const double nu = (double)act * a.avC * a.hEl[e] / (double)N * (double)lam;
+    sm.nu = (R)nu;
+    a.nu[e] = nu;
+    a.act[e] = (float)act;
+  }
+  __syncthreads();
+  // BR1 gradient (GradientBR_MappedScalar2D, src/SELF_MappedData.f90:990-1074) scaled by nu,
+  // and the contravariant viscous flux (src/models/hip/SELF_Advection2D.cpp:66-95)
+  if (live) {
+    const R nu = sm.nu;
+    const double* nH = a.nHat + 2 * (long long)P * 4 * e;
+    const double* nS = a.nScale + (long long)P * 4 * e;
+    const R Jij = (R)a.J[t + (long long)PP * e];
+    R* visc = reinterpret_cast<R*>(a.visc);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      R gx = (R)0, gy = (R)0;
+#pragma unroll
+      for (int ii = 0; ii < P; ++ii) {
+        const R qa = sm.q[v][ii + P * j], qb = sm.q[v][i + P * ii];
+        R f1 = qa * sm.dsdx[0][ii + P * j];
+        R f2 = qb * sm.dsdx[2][i + P * ii];
+        gx = gx + (R)sdg[ii + P * i] * f1 + (R)sdg[ii + P * j] * f2;
+        f1 = qa * sm.dsdx[1][ii + P * j];
+        f2 = qb * sm.dsdx[3][i + P * ii];
+        gy = gy + (R)sdg[ii + P * i] * f1 + (R)sdg[ii + P * j] * f2;
+      }
+      // nHat(d, k, side) at nH[d + 2 (k + P side)], nScale(k, side) at nS[k + P side]
+      R f1 = sm.avg[1][v][j] * (R)nH[0 + 2 * (j + P * 1)] * (R)nS[j + P * 1];
+      R f2 = sm.avg[3][v][j] * (R)nH[0 + 2 * (j + P * 3)] * (R)nS[j + P * 3];
+      gx = gx + (f1 * (R)sb[i + P] + f2 * (R)sb[i]) / (R)sw[i];
+      f1 = sm.avg[2][v][i] * (R)nH[0 + 2 * (i + P * 2)] * (R)nS[i + P * 2];
+      f2 = sm.avg[0][v][i] * (R)nH[0 + 2 * (i + P * 0)] * (R)nS[i + P * 0];
+      gx = gx + (f1 * (R)sb[j + P] + f2 * (R)sb[j]) / (R)sw[j];
+      f1 = sm.avg[1][v][j] * (R)nH[1 + 2 * (j + P * 1)] * (R)nS[j + P * 1];
+      f2 = sm.avg[3][v][j] * (R)nH[1 + 2 * (j + P * 3)] * (R)nS[j + P * 3];
+      gy = gy + (f1 * (R)sb[i + P] + f2 * (R)sb[i]) / (R)sw[i];
+      f1 = sm.avg[2][v][i] * (R)nH[1 + 2 * (i + P * 2)] * (R)nS[i + P * 2];
+      f2 = sm.avg[0][v][i] * (R)nH[1 + 2 * (i + P * 0)] * (R)nS[i + P * 0];
+      gy = gy + (f1 * (R)sb[j + P] + f2 * (R)sb[j]) / (R)sw[j];
+      gx = gx / Jij;
+      gy = gy / Jij;
+      gx = gx * nu;
+      gy = gy * nu;
+      sm.g[0][v][t] = gx;
+      sm.g[1][v][t] = gy;
+      const R c1 = -(sm.dsdx[0][t] * gx + sm.dsdx[1][t] * gy);
+      const R c2 = -(sm.dsdx[2][t] * gx + sm.dsdx[3][t] * gy);
+      visc[t + (long long)PP * (0 + 2 * (v + 4 * e))] = c1;
+      visc[t + (long long)PP * (1 + 2 * (v + 4 * e))] = c2;
+    }
+  }
+  __syncthreads();
+  // face traces of nu grad q (VectorBoundaryInterp_2D, src/SELF_Lagrange.f90:2284-2316)
+  if (live) {
+    R* vo = reinterpret_cast<R*>(a.vtr) + (long long)4 * VS * e;
+    for (int k = t; k < 4 * 8 * P; k += PP) {
+      const int ii = k % P, d = (k / P) % 2, v = (k / (2 * P)) % 4, s1 = k / (8 * P);
+      vo[s1 * VS + ii + P * (d + 2 * v)] = face_trace<P, R>(sm.g[d][v], sb, s1, ii);
+    }
+  }
+}
+
+// Closure features of a stored FP64 state (training-data harvest): per element
+// the indicator activation and the 36 features.
+template <int P>
+__global__ void __launch_bounds__(P* P) k_closure_features(const double* __restrict__ q, int nEl, AvArgs a,
+                                                            float* __restrict__ act, float* __restrict__ feat) {
+  constexpr int PP = P * P;
+  __shared__ double sq[2][PP], tt[2][PP], cc[2][PP], sT[PP];
+  const int t = threadIdx.x, i = t % P, j = t / P;
+  const long long e = blockIdx.x;
+  if (e >= nEl) return;
+  sT[t] = a.T[t];
+  sq[0][t] = q[t + (long long)PP * (2 + 4 * e)];
+  sq[1][t] = q[t + (long long)PP * (3 + 4 * e)];
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    double acc = 0.0;
+    for (int m = 0; m < P; ++m) acc = acc + sT[i + P * m] * sq[r][m + P * j];
+    tt[r][i + P * j] = acc;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    double acc = 0.0;
+    for (int m = 0; m < P; ++m) acc = acc + sT[j + P * m] * tt[r][i + P * m];
+    cc[r][i + P * j] = acc;
+  }
+  __syncthreads();
+  if (t == 0 && act) act[e] = (float)modal_activation<P, double>(cc[0], a.s0, a.kappa);
+  if constexpr (P >= 6) {
+    if (t < 2 && feat) modal_features<P, double>(cc[t], feat + kMlpIn * e + 18 * t);
+  }
+}
+
+struct QwArr {
+  double w[kMaxP];
+};
+
+template <typename R>
+cudaError_t launch_av_prep_impl(int P, const AvArgs& a, cudaStream_t st) {
+  switch (P) {
+#define SG_AV_CASE(PV)                                                                         \
+  case PV: {                                                                                   \
+    constexpr int EPB = av_elems_per_block<PV, R>();                                           \
+    k_av_prep<PV, R, EPB><<<(a.nEl + EPB - 1) / EPB, EPB * PV * PV, 0, st>>>(a);                \
+    return cudaGetLastError();                                                                 \
+  }
+    SG_AV_CASE(2)
+    SG_AV_CASE(3)
+    SG_AV_CASE(4)
+    SG_AV_CASE(5)
+    SG_AV_CASE(6)
+    SG_AV_CASE(7)
+    SG_AV_CASE(8)
+#undef SG_AV_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace selfgpu

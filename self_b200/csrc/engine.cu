@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "av_closure.cuh"
 #include "fused_stage.cuh"
 #include "selfgpu_internal.h"
 
@@ -54,11 +55,45 @@ struct selfgpu_model2d {
   // graph cache: one captured RK step per starting buffer parity
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   long long graphTma[2][2] = {{0, 0}, {0, 0}};
+  long long graphLaunches[2][2] = {{0, 0}, {0, 0}};
   double graphDt = NAN;
+  // artificial-viscosity closure (CIG): mode, per-launch arguments and buffers
+  int avMode = AV_OFF;
+  AvArgs av{};
+  double* avNu = nullptr;
+  float* avAct = nullptr;  // [0, nEl): activation applied, [nEl, 2 nEl): indicator activation
+  int* avFallbacks = nullptr;
+  double* avH = nullptr;
+  void* avVisc = nullptr;
+  void* avVtr = nullptr;
+  __nv_bfloat16* mlpW = nullptr;
+  float* mlpB = nullptr;
 
   size_t elemBytes() const { return form == SELFGPU_FP64 ? sizeof(double) : sizeof(float); }
 
+  // closure preparation of one stage: element viscosity, BR1 gradient, viscous
+  // volume flux and traces, from the solution and the trace cache trIn
+  cudaError_t launch_av(const void* trIn) {
+    AvArgs x = av;
+    x.nEl = nEl;
+    x.q = base.q;
+    x.dsdx = base.dsdx;
+    x.J = base.J;
+    x.nHat = base.nHat;
+    x.nScale = base.nScale;
+    x.sideInfo = base.sideInfo;
+    x.trIn = trIn;
+    x.presc = base.fld[2];
+    x.gamma = base.gamma;
+    ++launches;
+    return form == SELFGPU_FP64 ? launch_av_prep_fp64(P, x, stream) : launch_av_prep_fp32(P, x, stream);
+  }
+
   cudaError_t launch(StageArgs a) {
+    if (avMode != AV_OFF && a.mode != MODE_TRACES) {
+      cudaError_t e = launch_av(a.trIn);
+      if (e != cudaSuccess) return e;
+    }
     ++launches;
     int tma = 0;
     cudaError_t e = form == SELFGPU_FP64 ? launch_stage_fp64(model, P, a, cfg, stream, &tma)
@@ -188,6 +223,9 @@ int selfgpu_model2d_destroy(selfgpu_model2d* m) {
     if (m->tr[k]) cudaFree(m->tr[k]);
     if (m->vel[k]) cudaFree(m->vel[k]);
   }
+  for (void* p : {(void*)m->avNu, (void*)m->avAct, (void*)m->avFallbacks, (void*)m->avH, m->avVisc, m->avVtr,
+                  (void*)m->mlpW, (void*)m->mlpB})
+    if (p) cudaFree(p);
   if (m->dflag) cudaFree(m->dflag);
   if (m->ownStream) cudaStreamDestroy(m->stream);
   delete m;
@@ -340,6 +378,7 @@ int selfgpu_model2d_rk3(selfgpu_model2d* m, double dt, int nSteps) {
           const long long l0 = m->launches, t0 = m->tmaLaunches;
           e = m->step(dt);
           m->graphTma[c0][v0] = m->tmaLaunches - t0;
+          m->graphLaunches[c0][v0] = m->launches - l0;
           m->launches = l0;
           m->tmaLaunches = t0;
           cudaError_t e2 = cudaStreamEndCapture(m->stream, &graph);
@@ -364,7 +403,7 @@ int selfgpu_model2d_rk3(selfgpu_model2d* m, double dt, int nSteps) {
     }
     e = cudaGraphLaunch(g, m->stream);
     if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_rk3: graph launch", e);
-    m->launches += 3;
+    m->launches += m->graphLaunches[m->cur][m->vcur];
     m->tmaLaunches += m->graphTma[m->cur][m->vcur];
     m->cur = 1 - m->cur;  // three swaps per step
     if (m->model == SELFGPU_MODEL_SW) m->vcur = 1 - m->vcur;
@@ -438,6 +477,13 @@ int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, f
     a.velIn = m->vel[m->vcur];
     a.velOut = m->vel[1 - m->vcur];  // written, not consumed: the cache parity is left unchanged
   }
+  if (m->avMode != AV_OFF) {
+    e = m->launch_av(a.trIn);  // the candidates then read this state's viscous terms
+    if (e != cudaSuccess) {
+      cudaFree(scratch);
+      return fail_cuda("selfgpu_model2d_autotune", e);
+    }
+  }
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
@@ -483,6 +529,122 @@ int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, f
   if (persistent) *persistent = bestCfg.allowTma ? 1 : 0;
   if (groups) *groups = bestCfg.allowTma ? bestCfg.maxGroups : 0;
   if (usPerStage) *usPerStage = best * 1000.f / 3.f;
+  return SELFGPU_OK;
+}
+
+int selfgpu_model2d_set_closure(selfgpu_model2d* m, int mode, double c, double s0, double kappa,
+                                const double* controlPoints) {
+  if (!m) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_closure: null handle");
+  if (mode == AV_OFF) {
+    m->avMode = AV_OFF;
+    m->base.av = 0;
+    m->drop_graphs();
+    return SELFGPU_OK;
+  }
+  if (m->model != SELFGPU_MODEL_CIG)
+    return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_closure: the closure is defined for CompressibleIdealGas2D");
+  if (mode != AV_INDICATOR && mode != AV_MLP)
+    return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_closure: unknown closure mode");
+  if (mode == AV_MLP && (m->P < 6 || !m->mlpW))
+    return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_closure: the MLP closure needs N >= 5 and weights "
+                                      "(selfgpu_model2d_set_mlp)");
+  if (!controlPoints || !(kappa > 0.0) || !(c >= 0.0))
+    return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_closure: bad arguments");
+  if (!m->haveInterp || !m->haveGeometry)
+    return set_error(SELFGPU_ERR_STATE, "selfgpu_model2d_set_closure: interp and geometry must be set first");
+  const size_t nEl = (size_t)m->nEl, PP = (size_t)m->P * m->P;
+  cudaError_t e = cudaSuccess;
+  if (!m->avNu) {
+    e = cudaMalloc(&m->avNu, nEl * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&m->avAct, 2 * nEl * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&m->avFallbacks, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&m->avH, nEl * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&m->avVisc, 8 * PP * nEl * m->elemBytes());
+    if (e == cudaSuccess) e = cudaMalloc(&m->avVtr, 4 * 8 * (size_t)m->P * nEl * m->elemBytes());
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->avFallbacks, 0, sizeof(int), m->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->avAct, 0, 2 * nEl * sizeof(float), m->stream);
+    if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_set_closure", e);
+  }
+  AvArgs& x = m->av;
+  x.mode = mode;
+  x.avC = c;
+  x.s0 = s0;
+  x.kappa = kappa;
+  modal_matrix(m->N, controlPoints, m->base.qw, x.T);
+  std::memcpy(x.dgM, m->base.dgM, sizeof(x.dgM));
+  std::memcpy(x.bM, m->base.bM, sizeof(x.bM));
+  std::memcpy(x.qw, m->base.qw, sizeof(x.qw));
+  x.hEl = m->avH;
+  x.nu = m->avNu;
+  x.act = m->avAct;
+  x.actInd = m->avAct + nEl;
+  x.fallbacks = m->avFallbacks;
+  x.visc = m->avVisc;
+  x.vtr = m->avVtr;
+  x.mlpW = m->mlpW;
+  x.mlpB = m->mlpB;
+  e = launch_element_size(m->base.J, m->base.qw, m->P, m->nEl, m->avH, m->stream);
+  if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_set_closure", e);
+  m->avMode = mode;
+  m->base.av = 1;
+  m->base.visc = m->avVisc;
+  m->base.vtr = m->avVtr;
+  m->drop_graphs();
+  return SELFGPU_OK;
+}
+
+int selfgpu_model2d_set_mlp(selfgpu_model2d* m, const uint16_t* weights, const float* params) {
+  if (!m || !weights || !params) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_mlp: null argument");
+  cudaError_t e = cudaSuccess;
+  if (!m->mlpW) {
+    e = cudaMalloc(&m->mlpW, kMlpWeights * sizeof(__nv_bfloat16));
+    if (e == cudaSuccess) e = cudaMalloc(&m->mlpB, kMlpFloats * sizeof(float));
+    if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_set_mlp", e);
+  }
+  e = cudaMemcpyAsync(m->mlpW, weights, kMlpWeights * sizeof(uint16_t), cudaMemcpyHostToDevice, m->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(m->mlpB, params, kMlpFloats * sizeof(float), cudaMemcpyHostToDevice, m->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+  if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_set_mlp", e);
+  m->av.mlpW = m->mlpW;
+  m->av.mlpB = m->mlpB;
+  m->drop_graphs();
+  return SELFGPU_OK;
+}
+
+int selfgpu_model2d_closure_state(selfgpu_model2d* m, double* nu, float* activation, float* indicatorActivation,
+                                  int* fallbacks, int resetFallbacks) {
+  if (!m) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_closure_state: null handle");
+  if (!m->avNu) return set_error(SELFGPU_ERR_STATE, "selfgpu_model2d_closure_state: no closure has been set");
+  const size_t nEl = (size_t)m->nEl;
+  cudaError_t e = cudaSuccess;
+  if (nu) e = cudaMemcpyAsync(nu, m->avNu, nEl * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);
+  if (e == cudaSuccess && activation)
+    e = cudaMemcpyAsync(activation, m->avAct, nEl * sizeof(float), cudaMemcpyDeviceToDevice, m->stream);
+  if (e == cudaSuccess && indicatorActivation)
+    e = cudaMemcpyAsync(indicatorActivation, m->avAct + nEl, nEl * sizeof(float), cudaMemcpyDeviceToDevice,
+                        m->stream);
+  if (e == cudaSuccess && fallbacks) {
+    e = cudaMemcpyAsync(fallbacks, m->avFallbacks, sizeof(int), cudaMemcpyDeviceToHost, m->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+  }
+  if (e == cudaSuccess && resetFallbacks) e = cudaMemsetAsync(m->avFallbacks, 0, sizeof(int), m->stream);
+  if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_closure_state", e);
+  return SELFGPU_OK;
+}
+
+int selfgpu_cig2d_closure_features(const double* q, int N, int nEl, const double* controlPoints,
+                                   const double* qWeights, double s0, double kappa, float* activation,
+                                   float* features, void* stream) {
+  if (!q || N < 1 || N > SELFGPU_MAX_N || nEl < 1 || !controlPoints || !qWeights || !(kappa > 0.0))
+    return set_error(SELFGPU_ERR_ARG, "selfgpu_cig2d_closure_features: bad arguments");
+  if (features && N < 5) return set_error(SELFGPU_ERR_ARG, "selfgpu_cig2d_closure_features: features need N >= 5");
+  AvArgs x{};
+  x.s0 = s0;
+  x.kappa = kappa;
+  modal_matrix(N, controlPoints, qWeights, x.T);
+  cudaError_t e = launch_closure_features(q, N + 1, nEl, x, activation, features, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail_cuda("selfgpu_cig2d_closure_features", e);
   return SELFGPU_OK;
 }
 

@@ -66,6 +66,12 @@ struct StageArgs {
   // rk_g * dtElem[e] when a per-element time step is bound (ensembles)
   double rk_a, rk_gdt, rk_g;
   const double* dtElem;
+  // artificial-viscosity closure (CIG; av_closure.cuh): contravariant viscous
+  // volume flux (P*P, 2, 4, nEl) and per (element, side) face traces of
+  // nu grad q (8P values at [i + P (d + 2 v)]), both bulk type
+  int av;
+  const void* visc;
+  const void* vtr;
   // bounded waits of the persistent kernel (clock cycles) and its error word
   long long waitCycles;
   int* err;
@@ -272,6 +278,46 @@ __device__ __forceinline__ void face_aux_global(const StageArgs& s, int side, in
   }
 }
 
+// Viscous closure terms (CompressibleIdealGas2D only).  Volume: the
+// contravariant viscous flux is added to the contravariant inviscid flux.
+// Face: on exchanged sides -1/2 (nu grad q_in + nu grad q_ex) . n nScale is
+// added to the Riemann flux, the exterior value taken from the neighbour's
+// traces with the flip applied (src/models/hip/SELF_Advection2D.cpp:140-175
+// with one viscosity per element); physical sides carry no viscous flux.
+template <int P>
+__host__ __device__ constexpr int visc_side_stride() {
+  return 8 * P;  // 2 components x 4 variables x P nodes
+}
+
+template <int P, typename R>
+__device__ __forceinline__ void av_volume_add(const StageArgs& s, int t, long long e, R* F0, R* F1) {
+  constexpr int PP = P * P;
+  const R* vs = reinterpret_cast<const R*>(s.visc) + t + (long long)PP * 8 * e;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    F0[v] = F0[v] + vs[PP * (0 + 2 * v)];
+    F1[v] = F1[v] + vs[PP * (1 + 2 * v)];
+  }
+}
+
+template <int P, typename R>
+__device__ __forceinline__ void av_face_add(const StageArgs& s, int s1, int ii, long long e, const int* si,
+                                            double n1, double n2, double nmag, R out[4]) {
+  constexpr int VS = visc_side_stride<P>(), N = P - 1;
+  const R* vt = reinterpret_cast<const R*>(s.vtr);
+  if (si[4] != 0) return;
+  const R* own = vt + (long long)VS * (s1 + 4 * e);
+  const long long e2 = si[2] - 1;
+  const R* ext = vt + (long long)VS * (si[3] / 10 - 1 + 4 * e2);
+  const int ie = (si[3] % 10) ? N - ii : ii;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    const R in = own[ii + P * (0 + 2 * v)] * (R)n1 + own[ii + P * (1 + 2 * v)] * (R)n2;
+    const R ex = ext[ie + P * (0 + 2 * v)] * (R)n1 + ext[ie + P * (1 + 2 * v)] * (R)n2;
+    out[v] = out[v] + (R)(-0.5) * (in + ex) * (R)nmag;
+  }
+}
+
 // Boundary interpolation of one traced field at face node ii of side s1
 // (src/SELF_Lagrange.f90:2241-2270): S and N run along j at fixed i, E and W
 // along i at fixed j.
@@ -359,10 +405,18 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
       Phys::template flux<R>(f, na, a, Fx, Fy);
       const double2* gp = reinterpret_cast<const double2*>(a.dsdx + 4 * gnode);
       const double2 c1 = gp[0], c2 = gp[1];  // (dsdx11, dsdx21), (dsdx12, dsdx22)
+      R F0[NV], F1[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        sm.Fc[0][v][t] = (R)c1.x * Fx[v] + (R)c1.y * Fy[v];
-        sm.Fc[1][v][t] = (R)c2.x * Fx[v] + (R)c2.y * Fy[v];
+        F0[v] = (R)c1.x * Fx[v] + (R)c1.y * Fy[v];
+        F1[v] = (R)c2.x * Fx[v] + (R)c2.y * Fy[v];
+      }
+      if constexpr (NV == 4)
+        if (a.av) av_volume_add<P, R>(a, t, e, F0, F1);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        sm.Fc[0][v][t] = F0[v];
+        sm.Fc[1][v][t] = F1[v];
       }
       for (int k = t; k < 4 * NT * P; k += PP) {
         const int ii = k % P, fs = k / P, fi = fs % NT, s1 = fs / NT;
@@ -434,6 +488,8 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
         }
         R out[NV];
         Phys::template face<R>(bcid, physical, L, X, velL, velR, nh.x, nh.y, ns, fx, a, out);
+        if constexpr (NV == 4)
+          if (a.av) av_face_add<P, R>(a, s1, ii, e, si, nh.x, nh.y, ns, out);
 #pragma unroll
         for (int v = 0; v < NV; ++v) sm.fb[s1][v][ii] = out[v];
       }

@@ -317,10 +317,18 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       Phys::template flux<R>(f, na, a, Fx, Fy);
       const double2* gp = reinterpret_cast<const double2*>(sl + pl.oDsdx) + 2 * t;
       const double2 c1 = gp[0], c2 = gp[1];
+      R F0[NV], F1[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        gU[v * PP + t] = (R)c1.x * Fx[v] + (R)c1.y * Fy[v];
-        gU[(NV + v) * PP + t] = (R)c2.x * Fx[v] + (R)c2.y * Fy[v];
+        F0[v] = (R)c1.x * Fx[v] + (R)c1.y * Fy[v];
+        F1[v] = (R)c2.x * Fx[v] + (R)c2.y * Fy[v];
+      }
+      if constexpr (NV == 4)
+        if (a.av) av_volume_add<P, R>(a, t, e, F0, F1);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        gU[v * PP + t] = F0[v];
+        gU[(NV + v) * PP + t] = F1[v];
       }
     }
 
@@ -376,6 +384,8 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       }
       R out[NV];
       Phys::template face<R>(bcid, physical, L, X, velL, velR, nh.x, nh.y, ns, fx, a, out);
+      if constexpr (NV == 4)
+        if (a.av) av_face_add<P, R>(a, s1, ii, e, ssi + 5 * s1, nh.x, nh.y, ns, out);
 #pragma unroll
       for (int v = 0; v < NV; ++v) gfb[(s1 * NV + v) * P + ii] = out[v];
     }

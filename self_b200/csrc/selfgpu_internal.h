@@ -21,6 +21,8 @@ int mesh2d_structured(int nx, int ny, double x0, double x1, double y0, double y1
                       double amp, int bcid, const int* rot, double* nodeCoords, int* globalNodeIDs,
                       int* sideInfo);
 int validate_side_info(const int* sideInfo, int nEl);
+// T(k,i) = w_i sqrt((2k+1)/2) L_k(x_i): nodal -> orthonormal Legendre modes
+void modal_matrix(int N, const double* x, const double* w, double* T);
 
 // Fused stage launches (stage_fp64.cu / stage_fp32.cu).
 struct StageArgs;
@@ -39,4 +41,11 @@ cudaError_t launch_stage_fp64(int model, int P, const StageArgs& a, const StageL
                               int* usedTma);
 cudaError_t launch_stage_fp32(int model, int P, const StageArgs& a, const StageLaunch& L, cudaStream_t st,
                               int* usedTma);
+// Artificial-viscosity closure (av_closure.cuh).
+struct AvArgs;
+cudaError_t launch_av_prep_fp64(int P, const AvArgs& a, cudaStream_t st);
+cudaError_t launch_av_prep_fp32(int P, const AvArgs& a, cudaStream_t st);
+cudaError_t launch_element_size(const double* J, const double* qw, int P, int nEl, double* h, cudaStream_t st);
+cudaError_t launch_closure_features(const double* q, int P, int nEl, const AvArgs& a, float* act, float* feat,
+                                    cudaStream_t st);
 }  // namespace selfgpu

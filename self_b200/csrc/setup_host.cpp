@@ -326,6 +326,16 @@ int validate_side_info(const int* sideInfo, int nEl) {
   return SELFGPU_OK;
 }
 
+void modal_matrix(int N, const double* x, const double* w, double* T) {
+  const int P = N + 1;
+  for (int i = 0; i < P; ++i)
+    for (int k = 0; k < P; ++k) {
+      double l, dl;
+      legendre(k, x[i], l, dl);
+      T[k + P * i] = (std::sqrt((2.0 * k + 1.0) / 2.0) * l) * w[i];
+    }
+}
+
 }  // namespace selfgpu
 
 // ------------------------------------------------------------------ C ABI
@@ -354,6 +364,13 @@ int selfgpu_mesh2d_structured(int nx, int ny, double x0, double x1, double y0, d
     return selfgpu::set_error(SELFGPU_ERR_ARG, "selfgpu_mesh2d_structured: null output");
   return selfgpu::mesh2d_structured(nx, ny, x0, x1, y0, y1, periodicX, periodicY, perturbation, bcid, rotation,
                                     nodeCoords, globalNodeIDs, sideInfo);
+}
+
+int selfgpu_modal_matrix(int N, const double* controlPoints, const double* qWeights, double* T) {
+  if (N < 0 || N > SELFGPU_MAX_N || !controlPoints || !qWeights || !T)
+    return selfgpu::set_error(SELFGPU_ERR_ARG, "selfgpu_modal_matrix: bad arguments");
+  selfgpu::modal_matrix(N, controlPoints, qWeights, T);
+  return SELFGPU_OK;
 }
 
 int selfgpu_validate_side_info(const int* sideInfo, int nEl) {

@@ -1,6 +1,7 @@
 // FP32-bulk instantiation of the fused stage kernels: fluxes, traces and the
 // divergence in float (with multiply-add contraction); metric terms, sources'
 // fields and the RK accumulation of the solution stay in double.
+#include "av_closure.cuh"
 #include "stage_dispatch.cuh"
 
 namespace selfgpu {
@@ -8,4 +9,5 @@ cudaError_t launch_stage_fp32(int model, int P, const StageArgs& a, const StageL
                               int* usedTma) {
   return launch_stage_impl<float>(model, P, a, L, st, usedTma);
 }
+cudaError_t launch_av_prep_fp32(int P, const AvArgs& a, cudaStream_t st) { return launch_av_prep_impl<float>(P, a, st); }
 }  // namespace selfgpu

@@ -82,3 +82,22 @@ def aux_fields(model, x, seed=0):
         return {"topography": h}
     phi = (0.5 * Y + 0.1 * X).reshape(P, P, nEl, order="F")
     return {"gravityPotential": phi, "drag": np.full((P, P, nEl), 0.05, order="F")}
+
+
+def shock_state(x, seed=0, width=0.01):
+    """CompressibleIdealGas2D state with an oblique smoothed shock (tanh of the
+    given width) and a smooth background: elements across the front activate
+    the closure fully, elements near it partly, the rest not at all."""
+    rng = np.random.default_rng(seed + 7)
+    X, Y = x[0, :, :, 0, :], x[1, :, :, 0, :]
+    P, nEl = X.shape[0], X.shape[2]
+    x0, sl = rng.uniform(0.4, 0.6), rng.uniform(0.1, 0.4)
+    s = np.tanh((X + sl * Y - x0 - 0.5 * sl) / width)
+    rho = 0.8 + 0.3 * s + 0.02 * np.sin(2 * np.pi * Y)
+    p = 0.9 + 0.4 * s
+    u = 0.2 - 0.1 * s
+    v = 0.1 + 0.05 * np.cos(2 * np.pi * X)
+    q = np.zeros((P, P, 4, nEl), order="F")
+    q[:, :, 0], q[:, :, 1], q[:, :, 2] = rho * u, rho * v, rho
+    q[:, :, 3] = p / 0.4 + 0.5 * rho * (u * u + v * v)
+    return q
