@@ -203,6 +203,185 @@ def run_forms(steps=20, err_steps=500, n_instances=256):
     return out
 
 
+def _events_ms(fn):
+    """Device time of fn() from CUDA events on the default (legacy) stream; the
+    engine handles below use blocking streams, which are ordered with it."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def _rel_l2(a, b):
+    import torch
+    d = float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+    return d if np.isfinite(d) else None
+
+
+def shock_band(x, rng):
+    """Smooth density wave (the C2 state) plus one seeded shock-tube band: in
+    |y - y0| < 0.05 a Sod-like tube (rho, p) = (1, 1) | (0.125, 0.1) at rest,
+    split at x = x0."""
+    import torch
+    X, Y = x[:, 0, :, :, 0], x[:, 0, :, :, 1]
+    x0, y0 = rng.uniform(0.3, 0.7, size=2)
+    rho = 1.0 + 0.1 * torch.sin(2 * np.pi * X) * torch.sin(2 * np.pi * Y)
+    u = torch.full_like(X, 0.5)
+    v = torch.full_like(X, 0.3)
+    p = torch.ones_like(X)
+    band = (Y - y0).abs() < 0.05
+    left = X < x0
+    rho = torch.where(band, torch.where(left, torch.ones_like(X), torch.full_like(X, 0.125)), rho)
+    p = torch.where(band, torch.where(left, torch.ones_like(X), torch.full_like(X, 0.1)), p)
+    u = torch.where(band, torch.zeros_like(X), u)
+    v = torch.where(band, torch.zeros_like(X), v)
+    q = torch.empty((X.shape[0], 4) + tuple(X.shape[1:]), device=X.device, dtype=torch.float64)
+    q[:, 0], q[:, 1], q[:, 2] = rho * u, rho * v, rho
+    q[:, 3] = p / (GAMMA - 1.0) + 0.5 * rho * (u * u + v * v)
+    return q
+
+
+def _closure_variant(mesh, geo, q0, form, mode, mlp, steps, dt, dof):
+    """One timed run from q0: DOF-updates/s, the final state and closure statistics."""
+    import self_b200 as S
+    model = S.CompressibleIdealGas2D(mesh, geo, form=form)
+    model.SetSolution(q0)
+    if mode:
+        model.SetClosure(mode, c=1.0, mlp=mlp)
+    model.ForwardStep(2, dt)  # captures the RK-step graph
+    model.Sync()
+    model.SetSolution(q0)
+    model.workSol.zero_()
+    l0 = model.LaunchCount()
+    if mode:
+        model.ClosureState(reset=True)
+    ms = _events_ms(lambda: model.ForwardStep(steps, dt))
+    res = {"value": dof * steps / (ms / 1e3), "unit": "DOF-updates/s", "ms_per_rk3_step": ms / steps,
+           "launches_per_rk3_step": (model.LaunchCount() - l0) / steps}
+    if mode:
+        nu, act, ind, fb = model.ClosureState(reset=True)
+        res["active_elements_last_stage"] = int((act > 0).sum())
+        if mode == S.CLOSURE_MLP:
+            res["fallback_fraction"] = fb / (3.0 * steps * model.nElem)
+            res["mean_abs_activation_diff_vs_indicator_last_stage"] = float((act - ind).abs().mean())
+    sol = model.solution.clone()
+    del model
+    return res, sol
+
+
+def run_closure_forms(n_problems=16, snapshots=4, c4_steps=50, c5_steps=100):
+    """The learned shock closure (form 4) and the large single solve with all
+    forms: training data from FP64 N=7 runs, training, the C4 workload
+    (CIG 256x256 N=5 FP32, seeded four-quadrant Riemann problem) and the C5
+    workload (CIG 512x512 N=7, smooth density wave + shock-tube band), plus
+    the C2 solve in the FP32-bulk form."""
+    import torch
+
+    import self_b200 as S
+    from self_b200 import closure as CL
+    out = {}
+    t0 = time.perf_counter()
+    data = CL.harvest(N_run=7, nx=128, n_problems=n_problems, snapshots=snapshots, steps_between=20, seed=0,
+                      N_sample=(5, 7))
+    torch.cuda.synchronize()
+    out["harvest"] = {"runs": f"{n_problems} seeded four-quadrant Riemann problems, CIG periodic 128x128 N=7 FP64 "
+                              f"with the indicator closure, {snapshots} snapshots 20 RK3 steps apart; states "
+                              f"interpolated to N=5 for the N=5 closure",
+                      "seconds": time.perf_counter() - t0}
+    mlps = {}
+    for d, (f, l) in sorted(data.items()):
+        m = CL.ClosureMLP(seed=d)
+        t1 = time.perf_counter()
+        loss = m.train(f, l, epochs=8, batch=8192, lr=2e-3, seed=d)
+        tt = time.perf_counter() - t1
+        pred = m.infer(f)
+        mlps[d] = m
+        out[f"training_N{d}"] = {"samples": int(f.shape[0]), "active_fraction": float((l > 0).float().mean()),
+                                 "epochs": 8, "batch": 8192, "mse_first_last": [float(loss[0]), float(loss[-1])],
+                                 "mean_abs_err_vs_indicator": float((pred - l).abs().mean()), "seconds": tt}
+    del data
+
+    # C4: 256 x 256, N = 5, FP32 bulk, seeded Riemann problem, learned closure
+    N4 = 5
+    interp = S.Lagrange(N4, S.GAUSS, N4, S.UNIFORM)
+    mesh = S.Mesh2D(256, 256, periodic=(True, True))
+    geo = S.SEMQuad(interp, mesh)
+    rng = np.random.Generator(np.random.PCG64(100))
+    q0 = CL.riemann_quadrants(geo.x, rng)
+    dof4 = 4 * (N4 + 1) ** 2 * mesh.nElem
+    probe = S.CompressibleIdealGas2D(mesh, geo)
+    dt4 = CL.stable_dt(probe, q0)
+    del probe
+    c4 = {"workload": f"CIG periodic 256x256 N=5, seeded four-quadrant Riemann problem, {c4_steps} RK3 steps, "
+                      f"dt={dt4:.3e}", "dof": dof4}
+    ref4 = None
+    for name, form, mode, mlp in (("fp64_indicator", S.FP64, S.CLOSURE_INDICATOR, None),
+                                  ("fp32_learned", S.FP32_BULK, S.CLOSURE_MLP, mlps[5]),
+                                  ("fp32_indicator", S.FP32_BULK, S.CLOSURE_INDICATOR, None),
+                                  ("fp64_no_closure", S.FP64, S.CLOSURE_OFF, None)):
+        res, sol = _closure_variant(mesh, geo, q0, form, mode, mlp, c4_steps, dt4, dof4)
+        if ref4 is None:
+            ref4 = sol
+        else:
+            res["rel_l2_vs_fp64_indicator"] = _rel_l2(sol, ref4)
+        c4[name] = res
+    c4["speedup_fp32_learned_vs_fp64_no_closure"] = c4["fp32_learned"]["value"] / c4["fp64_no_closure"]["value"]
+    out["c4_learned_closure"] = c4
+    del ref4, q0, geo, mesh
+
+    # C5: 512 x 512, N = 7, all forms
+    N5 = 7
+    interp = S.Lagrange(N5, S.GAUSS, N5, S.UNIFORM)
+    mesh = S.Mesh2D(512, 512, periodic=(True, True), perturbation=0.02)
+    geo = S.SEMQuad(interp, mesh)
+    rng = np.random.Generator(np.random.PCG64(200))
+    q0 = shock_band(geo.x, rng)
+    dof5 = 4 * (N5 + 1) ** 2 * mesh.nElem
+    probe = S.CompressibleIdealGas2D(mesh, geo)
+    dt5 = CL.stable_dt(probe, q0)
+    del probe
+    c5 = {"workload": f"CIG periodic 512x512 perturbed N=7, smooth density wave + shock-tube band, {c5_steps} RK3 "
+                      f"steps, dt={dt5:.3e}", "dof": dof5}
+    ref5 = None
+    for name, form, mode, mlp in (("fp64_indicator", S.FP64, S.CLOSURE_INDICATOR, None),
+                                  ("fp32_learned", S.FP32_BULK, S.CLOSURE_MLP, mlps[7]),
+                                  ("fp32_indicator", S.FP32_BULK, S.CLOSURE_INDICATOR, None),
+                                  ("fp64_no_closure", S.FP64, S.CLOSURE_OFF, None)):
+        res, sol = _closure_variant(mesh, geo, q0, form, mode, mlp, c5_steps, dt5, dof5)
+        if ref5 is None:
+            ref5 = sol
+        else:
+            res["rel_l2_vs_fp64_indicator"] = _rel_l2(sol, ref5)
+        c5[name] = res
+    c5["speedup_fp32_learned_vs_fp64_no_closure"] = c5["fp32_learned"]["value"] / c5["fp64_no_closure"]["value"]
+    out["c5_large_solve"] = c5
+    del ref5, q0, geo, mesh
+
+    # C2 in the FP32-bulk form (smooth: the closure stays off), error vs the FP64 engine
+    interp = S.Lagrange(N, S.GAUSS, N, S.UNIFORM)
+    mesh = S.Mesh2D(NX, NX, periodic=(True, True), perturbation=0.02)
+    geo = S.SEMQuad(interp, mesh)
+    q0 = initial_state(geo.x)
+    c = (GAMMA * 1.0 / (q0[:, 2].min())).sqrt().item()
+    dt = CFL * geo.CovariantArcMin() / (np.hypot(0.5, 0.3) + c)
+    c2 = {}
+    ref2 = None
+    for name, form in (("fp64", S.FP64), ("fp32_bulk", S.FP32_BULK)):
+        res, sol = _closure_variant(mesh, geo, q0, form, S.CLOSURE_OFF, None, STEPS_PER_SOLVE, dt, DOF)
+        if ref2 is None:
+            ref2 = sol
+        else:
+            res["rel_l2_vs_fp64"] = _rel_l2(sol, ref2)
+        c2[name] = res
+    c2["speedup_fp32_bulk_vs_fp64"] = c2["fp32_bulk"]["value"] / c2["fp64"]["value"]
+    out["c2_forms"] = c2
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -347,6 +526,7 @@ def run_engine(args, rank, world, local_rank):
     }
     if not args.no_forms:
         line["forms"] = run_forms()
+        line["forms"].update(run_closure_forms())
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     print(json.dumps(line), flush=True)

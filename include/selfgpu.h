@@ -305,6 +305,10 @@ long long selfgpu_model2d_persistent_launch_count(const selfgpu_model2d* m);
  * one-CTA-per-element-group kernel. */
 int selfgpu_model2d_set_kernel(selfgpu_model2d* m, int persistent);
 
+/* Explicit launch configuration (what the autotuner picks): persistent 0/1
+ * and the persistent kernel's consumer-group cap (0 = as many as fit). */
+int selfgpu_model2d_set_launch(selfgpu_model2d* m, int persistent, int groups);
+
 /* Autotuner: times the per-element-group kernel and the persistent kernel at
  * every consumer-group count that fits (elements in flight per CTA, each with
  * its double-buffered staging tile) on tendency launches over this handle's

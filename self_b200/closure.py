@@ -175,15 +175,16 @@ def harvest(N_run, nx, n_problems, snapshots, steps_between, seed=0, N_sample=No
     """Features and indicator labels from FP64 indicator-closure runs of seeded
     four-quadrant Riemann problems on a periodic nx x nx mesh at degree N_run,
     sampled every steps_between RK3 steps (snapshots times per problem), the
-    states interpolated to degree N_sample first when it differs.  Returns
-    float32 device tensors (n, 36), (n,)."""
-    N_sample = N_run if N_sample is None else N_sample
+    states interpolated to each sample degree first when it differs from
+    N_run.  N_sample is one degree (returns float32 device tensors (n, 36),
+    (n,)) or a tuple of degrees (returns {degree: (features, labels)})."""
+    degrees = (N_run,) if N_sample is None else (N_sample if isinstance(N_sample, (tuple, list)) else (N_sample,))
     rng = np.random.Generator(np.random.PCG64(seed))
     interp = A.Lagrange(N_run, A.GAUSS, N_run, A.UNIFORM)
     mesh = A.Mesh2D(nx, nx, periodic=(True, True))
     geo = A.SEMQuad(interp, mesh)
-    samp = A.Lagrange(N_sample, A.GAUSS, N_sample, A.UNIFORM)
-    feats, labels = [], []
+    samp = {d: A.Lagrange(d, A.GAUSS, d, A.UNIFORM) for d in degrees}
+    out = {d: ([], []) for d in degrees}
     for _ in range(n_problems):
         model = A.CompressibleIdealGas2D(mesh, geo, form=A.FP64, stream=stream)
         q0 = riemann_quadrants(geo.x, rng)
@@ -194,9 +195,14 @@ def harvest(N_run, nx, n_problems, snapshots, steps_between, seed=0, N_sample=No
             if s > 0:
                 model.ForwardStep(steps_between, dt)
                 model.Sync()
-            state = model.solution if N_sample == N_run else grid_interp(model.solution, N_run, N_sample)
-            act, feat = features(state, samp)
-            feats.append(feat)
-            labels.append(act)
+            for d in degrees:
+                state = model.solution if d == N_run else grid_interp(model.solution, N_run, d)
+                act, feat = features(state, samp[d])
+                out[d][0].append(feat)
+                out[d][1].append(act)
+        model.CheckFinite()
         del model
-    return torch.cat(feats), torch.cat(labels)
+    res = {d: (torch.cat(f), torch.cat(l)) for d, (f, l) in out.items()}
+    if isinstance(N_sample, (tuple, list)):
+        return res
+    return res[degrees[0]]

@@ -31,6 +31,34 @@ __global__ void k_nonfinite(const double* __restrict__ q, long long n, int* flag
     }
 }
 
+// One element's packed geometry record (geo_record_doubles<P>() doubles):
+// dsdx (4 P^2), nHat (8 P), nScale (4 P), J (P^2), then sideInfo's 20 ints.
+__global__ void k_pack_geometry(const double* __restrict__ dsdx, const double* __restrict__ nHat,
+                                const double* __restrict__ nScale, const double* __restrict__ J,
+                                const int* __restrict__ sideInfo, int P, int nEl, int rec, double* __restrict__ out) {
+  const int PP = P * P;
+  const long long total = (long long)rec * nEl;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
+    const long long e = k / rec;
+    int w = (int)(k - e * rec);
+    double v = 0.0;
+    if (w < 4 * PP) {
+      v = dsdx[4 * PP * e + w];
+    } else if ((w -= 4 * PP) < 8 * P) {
+      v = nHat[8 * P * e + w];
+    } else if ((w -= 8 * P) < 4 * P) {
+      v = nScale[4 * P * e + w];
+    } else if ((w -= 4 * P) < PP) {
+      v = J[PP * e + w];
+    } else {
+      w -= PP;  // sideInfo: two ints per double slot
+      int2 pr = make_int2(sideInfo[20 * e + 2 * w], sideInfo[20 * e + 2 * w + 1]);
+      v = __longlong_as_double(((long long)(unsigned)pr.y << 32) | (unsigned)pr.x);
+    }
+    out[k] = v;
+  }
+}
+
 int nt_of(int model) { return model == SELFGPU_MODEL_CIG ? 9 : 3; }
 int nv_of(int model) { return model == SELFGPU_MODEL_CIG ? 4 : 3; }
 
@@ -68,6 +96,7 @@ struct selfgpu_model2d {
   void* avVtr = nullptr;
   __nv_bfloat16* mlpW = nullptr;
   float* mlpB = nullptr;
+  double* geo = nullptr;  // packed geometry records (persistent kernel)
 
   size_t elemBytes() const { return form == SELFGPU_FP64 ? sizeof(double) : sizeof(float); }
 
@@ -224,7 +253,7 @@ int selfgpu_model2d_destroy(selfgpu_model2d* m) {
     if (m->vel[k]) cudaFree(m->vel[k]);
   }
   for (void* p : {(void*)m->avNu, (void*)m->avAct, (void*)m->avFallbacks, (void*)m->avH, m->avVisc, m->avVtr,
-                  (void*)m->mlpW, (void*)m->mlpB})
+                  (void*)m->mlpW, (void*)m->mlpB, (void*)m->geo})
     if (p) cudaFree(p);
   if (m->dflag) cudaFree(m->dflag);
   if (m->ownStream) cudaStreamDestroy(m->stream);
@@ -257,6 +286,23 @@ int selfgpu_model2d_set_geometry(selfgpu_model2d* m, const double* dsdx, const d
   m->base.nHat = nHat;
   m->base.nScale = nScale;
   m->base.sideInfo = sideInfo_d;
+  // Packed per-element geometry records for the persistent kernel, built on
+  // the legacy default stream after whatever produced the arrays, and waited
+  // for (set-up time): the caller's arrays stay the source of truth, and a
+  // caller that changes them calls set_geometry again.
+  const int P = m->P;
+  const int rec = 5 * P * P + 12 * P + 10;  // geo_record_doubles<P>()
+  cudaError_t e = cudaSuccess;
+  if (!m->geo) e = cudaMalloc(&m->geo, (size_t)rec * m->nEl * sizeof(double));
+  if (e == cudaSuccess) {
+    const long long total = (long long)rec * m->nEl;
+    const int blocks = (int)((total + 255) / 256 < 4096 ? (total + 255) / 256 : 4096);
+    k_pack_geometry<<<blocks, 256, 0, 0>>>(dsdx, nHat, nScale, J, sideInfo_d, P, m->nEl, rec, m->geo);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_set_geometry", e);
+  m->base.geo = m->geo;
   m->haveGeometry = true;
   m->valid = false;
   m->drop_graphs();
@@ -445,6 +491,14 @@ int selfgpu_model2d_inject_stall(selfgpu_model2d* m, int enable) {
 int selfgpu_model2d_set_kernel(selfgpu_model2d* m, int persistent) {
   if (!m) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_kernel: null handle");
   m->cfg.allowTma = persistent != 0;
+  m->drop_graphs();
+  return SELFGPU_OK;
+}
+
+int selfgpu_model2d_set_launch(selfgpu_model2d* m, int persistent, int groups) {
+  if (!m || groups < 0) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_launch: bad arguments");
+  m->cfg.allowTma = persistent != 0;
+  m->cfg.maxGroups = groups;
   m->drop_graphs();
   return SELFGPU_OK;
 }

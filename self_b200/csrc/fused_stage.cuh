@@ -72,6 +72,10 @@ struct StageArgs {
   int av;
   const void* visc;
   const void* vtr;
+  // engine-owned packed geometry: per element one contiguous record of
+  // geo_record_doubles<P>() doubles (dsdx, nHat, nScale, J, then sideInfo as
+  // 20 ints); read by the persistent kernel with one bulk copy
+  const double* geo;
   // bounded waits of the persistent kernel (clock cycles) and its error word
   long long waitCycles;
   int* err;
@@ -81,6 +85,13 @@ struct StageArgs {
   double bM[2 * kMaxP];
   double qw[kMaxP];
 };
+
+// Doubles in one element's packed geometry record: dsdx (4 P^2), nHat (8 P),
+// nScale (4 P), J (P^2), sideInfo (20 ints = 10 doubles).
+template <int P>
+__host__ __device__ constexpr int geo_record_doubles() {
+  return 5 * P * P + 12 * P + 10;
+}
 
 // Trace-cache block size (values of the bulk type) of one (element, side).
 template <int P, int NT, typename R>

@@ -2,13 +2,16 @@
 //
 // One CTA per SM.  Warp 0 is the producer: for every element the CTA owns it
 // issues 1-D bulk asynchronous copies (cp.async.bulk, the non-tensor TMA path)
-// of the element's contiguous blocks -- solution, RK register, dsdx, J, nHat,
-// nScale, sideInfo, model fields -- and of the four neighbour trace blocks
-// named by sideInfo, into a shared-memory buffer whose mbarrier counts the
-// bytes in.  The remaining warps form C consumer groups of TPE threads (one
+// of the element's contiguous blocks -- solution, the engine's packed
+// geometry record (dsdx, nHat, nScale, J, sideInfo), its own face traces and
+// the model fields -- into a shared-memory buffer whose mbarrier counts the
+// bytes in.  Bulk copies are issued one at a time by one lane: the number of
+// copy requests per element, not their bytes, limits the producer, so the
+// per-element pieces that live in separate arrays are packed into one record
+// at set-up.  The remaining warps form C consumer groups of TPE threads (one
 // thread per node); each group owns two buffers, so the copies for its next
-// element are in flight while it computes the current one.  No thread waits
-// on global-memory latency except the producer's batched sideInfo reads.
+// element are in flight while it computes the current one.  The face threads
+// load the neighbours' trace values themselves (coalesced plain loads).
 //
 // Every wait is bounded (StageArgs::waitCycles): on timeout the kernel records
 // an error word, stops issuing copies, waits (again bounded) for copies it has
@@ -68,9 +71,9 @@ __device__ __forceinline__ void named_bar(int id, int nthreads) {
 struct TmaPlan {
   int groups;      // consumer groups per CTA
   int slotBytes;   // bytes of one element buffer
-  int oQ, oDsdx, oNhat, oNs, oSi, oOwn, oNbr;
+  int oQ, oDsdx, oNhat, oNs, oJ, oSi, oOwn;  // oDsdx..oSi lie in the packed geometry record
   int oX[5];       // model fields: LSW (H, Hb, fC), SW (topoB, grad), CIG (envG, drag, presc x3 -> oX[2..4])
-  int oVelOwn, oVelNbr;
+  int oVelOwn;
   int oMats, oFlags, oSlots, oGroups, groupBytes, smemBytes;
 };
 
@@ -127,122 +130,67 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     const int lane = threadIdx.x & 31;
     bool abort = false;
     long long issued = 0;
-    const R* trIn = reinterpret_cast<const R*>(a.trIn);
-    const R* vIn = reinterpret_cast<const R*>(a.velIn);
-    for (long long k0 = 0; k0 < nMine && !abort; k0 += 32) {
-      // each lane fetches the connectivity of one element of this batch
-      int nbE[4] = {0, 0, 0, 0}, nbS[4] = {0, 0, 0, 0};  // e2 (1-based, 0 = none), s2 (0-based)
-      if (k0 + lane < nMine) {
-        const long long e = blockIdx.x + (k0 + lane) * gridDim.x;
-        const int4* si4 = reinterpret_cast<const int4*>(a.sideInfo + 20 * e);
-        int si[20];
-#pragma unroll
-        for (int q = 0; q < 5; ++q) {
-          const int4 v = si4[q];
-          si[4 * q] = v.x;
-          si[4 * q + 1] = v.y;
-          si[4 * q + 2] = v.z;
-          si[4 * q + 3] = v.w;
-        }
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-          if (si[5 * s + 4] == 0) {
-            nbE[s] = si[5 * s + 2];
-            nbS[s] = si[5 * s + 3] / 10 - 1;
-          }
-        }
+    if (lane == 0) {
+      const R* trIn = reinterpret_cast<const R*>(a.trIn);
+      const R* vIn = reinterpret_cast<const R*>(a.velIn);
+      const uint32_t qb = NV * PP * 8, gb = geo_record_doubles<P>() * 8, ob = 4 * TS * sizeof(R);
+      uint32_t xb[5] = {0, 0, 0, 0, 0};
+      if constexpr (kLSW) {
+        xb[0] = PP * 8;
+        xb[1] = 4 * P * 8;
+        xb[2] = a.fld[2] ? PP * 8 : 0;
+      } else if constexpr (kSW) {
+        xb[0] = a.fld[0] ? 4 * P * 8 : 0;
+        xb[1] = a.fld[1] ? 2 * PP * 8 : 0;
+      } else {
+        xb[0] = a.fld[0] ? 2 * PP * 8 : 0;
+        xb[1] = a.fld[1] ? PP * 8 : 0;
+        xb[2] = xb[3] = xb[4] = a.fld[2] ? 16 * P * 8 : 0;
       }
-      const int nb = (int)min(32LL, nMine - k0);
-      for (int b = 0; b < nb; ++b) {
-        int e2[4], s2[4];
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-          e2[s] = __shfl_sync(0xffffffffu, nbE[s], b);
-          s2[s] = __shfl_sync(0xffffffffu, nbS[s], b);
-        }
-        const long long k = k0 + b;
+      uint32_t bytes = qb + gb + ob + xb[0] + xb[1] + xb[2] + xb[3] + xb[4];
+      if constexpr (kSW) bytes += 8 * P * sizeof(R);
+      for (long long k = 0; k < nMine; ++k) {
         const int g = (int)(k % C);
         const long long jj = k / C;
         const int buf = (int)(jj & 1);
         const uint32_t par = (uint32_t)((jj >> 1) & 1);
-        if (lane == 0) {
-          if (!mbar_wait(&empty[2 * g + buf], par ^ 1u, a.waitCycles)) {
-            abort = true;
-          } else {
-            const long long e = blockIdx.x + k * gridDim.x;
-            unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
-            uint64_t* bar = &full[2 * g + buf];
-            const uint32_t qb = NV * PP * 8;
-            const uint32_t tsb = TS * sizeof(R);
-            const uint32_t vnb = 2 * P * sizeof(R);
-            int nInt = 0;
-#pragma unroll
-            for (int s = 0; s < 4; ++s) nInt += (e2[s] != 0);
-            uint32_t bytes = qb + 4 * PP * 8 + 8 * P * 8 + 4 * P * 8 + 80 + 4 * tsb + nInt * tsb;
-            if constexpr (kSW) bytes += 8 * P * sizeof(R) + nInt * vnb;
-            uint32_t xb[5] = {0, 0, 0, 0, 0};
-            if constexpr (kLSW) {
-              xb[0] = PP * 8;
-              xb[1] = 4 * P * 8;
-              xb[2] = a.fld[2] ? PP * 8 : 0;
-            } else if constexpr (kSW) {
-              xb[0] = a.fld[0] ? 4 * P * 8 : 0;
-              xb[1] = a.fld[1] ? 2 * PP * 8 : 0;
-            } else {
-              xb[0] = a.fld[0] ? 2 * PP * 8 : 0;
-              xb[1] = a.fld[1] ? PP * 8 : 0;
-              xb[2] = xb[3] = xb[4] = a.fld[2] ? 16 * P * 8 : 0;
-            }
-            for (int x = 0; x < 5; ++x) bytes += xb[x];
-            mbar_arrive_expect_tx(bar, bytes);
-            if (!(a.debugStarve && blockIdx.x == 0 && k == 0)) {
-              bulk_g2s(sl + pl.oQ, a.q + (size_t)e * NV * PP, qb, bar);
-              bulk_g2s(sl + pl.oDsdx, a.dsdx + (size_t)e * 4 * PP, 4 * PP * 8, bar);
-              bulk_g2s(sl + pl.oNhat, a.nHat + (size_t)e * 8 * P, 8 * P * 8, bar);
-              bulk_g2s(sl + pl.oNs, a.nScale + (size_t)e * 4 * P, 4 * P * 8, bar);
-              bulk_g2s(sl + pl.oSi, a.sideInfo + (size_t)e * 20, 80, bar);
-              bulk_g2s(sl + pl.oOwn, trIn + (size_t)4 * TS * e, 4 * tsb, bar);
-#pragma unroll
-              for (int s = 0; s < 4; ++s)
-                if (e2[s] != 0)
-                  bulk_g2s(sl + pl.oNbr + s * tsb, trIn + (size_t)TS * (s2[s] + 4 * (size_t)(e2[s] - 1)), tsb, bar);
-              if constexpr (kSW) {
-                bulk_g2s(sl + pl.oVelOwn, vIn + (size_t)e * 8 * P, 8 * P * sizeof(R), bar);
-#pragma unroll
-                for (int s = 0; s < 4; ++s)
-                  if (e2[s] != 0)
-                    bulk_g2s(sl + pl.oVelNbr + s * vnb, vIn + (size_t)2 * P * (s2[s] + 4 * (size_t)(e2[s] - 1)), vnb,
-                             bar);
-              }
-              if constexpr (kLSW) {
-                bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * PP, xb[0], bar);
-                bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 4 * P, xb[1], bar);
-                if (xb[2]) bulk_g2s(sl + pl.oX[2], a.fld[2] + (size_t)e * PP, xb[2], bar);
-              } else if constexpr (kSW) {
-                if (xb[0]) bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * 4 * P, xb[0], bar);
-                if (xb[1]) bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 2 * PP, xb[1], bar);
-              } else {
-                if (xb[0]) bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * 4 * PP, xb[0], bar);
-                if (xb[1]) bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 2 * PP + PP, xb[1], bar);
-                if (xb[2])
-                  for (int x = 2; x < 5; ++x) bulk_g2s(sl + pl.oX[x], a.fld[x] + (size_t)e * 16 * P, xb[x], bar);
-              }
-            }
-            issued = k + 1;
-          }
+        if (!mbar_wait(&empty[2 * g + buf], par ^ 1u, a.waitCycles)) {
+          abort = true;
+          break;
         }
-        abort = __shfl_sync(0xffffffffu, abort ? 1 : 0, 0) != 0;
-        if (abort) break;
+        const long long e = blockIdx.x + k * gridDim.x;
+        unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
+        uint64_t* bar = &full[2 * g + buf];
+        mbar_arrive_expect_tx(bar, bytes);
+        issued = k + 1;
+        if (a.debugStarve && blockIdx.x == 0 && k == 0) continue;
+        bulk_g2s(sl + pl.oQ, a.q + (size_t)e * NV * PP, qb, bar);
+        bulk_g2s(sl + pl.oDsdx, a.geo + (size_t)e * geo_record_doubles<P>(), gb, bar);
+        bulk_g2s(sl + pl.oOwn, trIn + (size_t)4 * TS * e, ob, bar);
+        if constexpr (kSW) bulk_g2s(sl + pl.oVelOwn, vIn + (size_t)e * 8 * P, 8 * P * sizeof(R), bar);
+        if constexpr (kLSW) {
+          bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * PP, xb[0], bar);
+          bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 4 * P, xb[1], bar);
+          if (xb[2]) bulk_g2s(sl + pl.oX[2], a.fld[2] + (size_t)e * PP, xb[2], bar);
+        } else if constexpr (kSW) {
+          if (xb[0]) bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * 4 * P, xb[0], bar);
+          if (xb[1]) bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 2 * PP, xb[1], bar);
+        } else {
+          if (xb[0]) bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * 4 * PP, xb[0], bar);
+          if (xb[1]) bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 2 * PP + PP, xb[1], bar);
+          if (xb[2])
+            for (int x = 2; x < 5; ++x) bulk_g2s(sl + pl.oX[x], a.fld[x] + (size_t)e * 16 * P, xb[x], bar);
+        }
       }
-    }
-    if (lane == 0 && abort) {
-      if (a.err) atomicExch(a.err, 1);
-      // Wait (bounded) for the copies already issued into buffers no consumer
-      // will read any more, so none is in flight when the CTA exits.
-      for (long long k = (issued > 2 * C ? issued - 2 * C : 0); k < issued; ++k) {
-        const int g = (int)(k % C);
-        const long long jj = k / C;
-        mbar_wait(&full[2 * g + (int)(jj & 1)], (uint32_t)((jj >> 1) & 1), a.waitCycles);
+      if (abort) {
+        if (a.err) atomicExch(a.err, 1);
+        // Wait (bounded) for the copies already issued into buffers no consumer
+        // will read any more, so none is in flight when the CTA exits.
+        for (long long k = (issued > 2 * C ? issued - 2 * C : 0); k < issued; ++k) {
+          const int g = (int)(k % C);
+          const long long jj = k / C;
+          mbar_wait(&full[2 * g + (int)(jj & 1)], (uint32_t)((jj >> 1) & 1), a.waitCycles);
+        }
       }
     }
     return;
@@ -266,11 +214,10 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     const int buf = (int)(jj & 1);
     const uint32_t par = (uint32_t)((jj >> 1) & 1);
     const unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
-    // RK register and Jacobian straight from global memory; they are first
-    // used after the face phase, which hides the latency.
-    double Gv[NV], Jij = 1.0;
+    // RK register straight from global memory; it is first used after the
+    // face phase, which hides the latency.
+    double Gv[NV];
     if (active) {
-      Jij = a.J[t + (size_t)PP * e];
       if (rk) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) Gv[v] = a.G[t + (size_t)PP * (v + NV * (size_t)e)];
@@ -285,10 +232,11 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     const int* ssi = reinterpret_cast<const int*>(sl + pl.oSi);
 
     // ---- A: solution (kept in registers), flux auxiliaries, contravariant flux
-    double qv[NV];
+    double qv[NV], Jij = 1.0;
     R f[NF];
     double na[3] = {0.0, 0.0, 0.0};
     if (active) {
+      Jij = reinterpret_cast<const double*>(sl + pl.oJ)[t];  // read before the buffer is released
       const double* sq = reinterpret_cast<const double*>(sl + pl.oQ);
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
@@ -339,13 +287,15 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       const bool physical = (bcid != 0) && (ssi[5 * s1 + 2] == 0);
       const int flip = ssi[5 * s1 + 3] % 10;
       const R* own = reinterpret_cast<const R*>(sl + pl.oOwn) + s1 * TS;
-      const R* nbr = reinterpret_cast<const R*>(sl + pl.oNbr) + s1 * TS;
       const int i2 = flip ? N - ii : ii;
+      const long long nb = (bcid == 0) ? (long long)TS * (ssi[5 * s1 + 3] / 10 - 1 + 4 * (long long)(ssi[5 * s1 + 2] - 1))
+                                       : -1;
+      const R* nbr = reinterpret_cast<const R*>(a.trIn) + (nb < 0 ? 0 : nb);
       R L[NT], X[NT];
 #pragma unroll
       for (int kf = 0; kf < NT; ++kf) {
         L[kf] = own[ii + P * kf];
-        X[kf] = (bcid == 0) ? nbr[i2 + P * kf] : (R)0;
+        X[kf] = (nb >= 0) ? nbr[i2 + P * kf] : (R)0;
       }
       const double2 nh = reinterpret_cast<const double2*>(sl + pl.oNhat)[ii + P * s1];
       const double ns = reinterpret_cast<const double*>(sl + pl.oNs)[ii + P * s1];
@@ -373,8 +323,9 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         const R* vo = reinterpret_cast<const R*>(sl + pl.oVelOwn);
         velL[0] = vo[ii + P * (0 + 2 * s1)];
         velL[1] = vo[ii + P * (1 + 2 * s1)];
-        if (bcid == 0) {
-          const R* vn = reinterpret_cast<const R*>(sl + pl.oVelNbr + s1 * 2 * P * sizeof(R));
+        if (nb >= 0) {  // the neighbour's stage-lagged velocity traces, plain loads
+          const R* vn = reinterpret_cast<const R*>(a.velIn) +
+                        (size_t)2 * P * (ssi[5 * s1 + 3] / 10 - 1 + 4 * (size_t)(ssi[5 * s1 + 2] - 1));
           velR[0] = vn[i2];
           velR[1] = vn[i2 + P];
         }
@@ -461,15 +412,16 @@ inline bool make_tma_plan(const StageArgs& a, int smemLimit, TmaPlan& pl, int ma
     o += (bytes + 15) / 16 * 16;
     return at;
   };
+  if (!a.geo) return false;
   pl.oQ = put(NV * PP * 8);
-  pl.oDsdx = put(4 * PP * 8);
-  pl.oNhat = put(8 * P * 8);
-  pl.oNs = put(4 * P * 8);
-  pl.oSi = put(80);
+  pl.oDsdx = put(geo_record_doubles<P>() * 8);  // packed record: dsdx, nHat, nScale, J, sideInfo
+  pl.oNhat = pl.oDsdx + 4 * PP * 8;
+  pl.oNs = pl.oNhat + 8 * P * 8;
+  pl.oJ = pl.oNs + 4 * P * 8;
+  pl.oSi = pl.oJ + PP * 8;
   pl.oOwn = put(4 * TS * (int)sizeof(R));
-  pl.oNbr = put(4 * TS * (int)sizeof(R));
   for (int x = 0; x < 5; ++x) pl.oX[x] = -1;
-  pl.oVelOwn = pl.oVelNbr = -1;
+  pl.oVelOwn = -1;
   if (kLSW) {
     pl.oX[0] = put(PP * 8);
     pl.oX[1] = put(4 * P * 8);
@@ -478,7 +430,6 @@ inline bool make_tma_plan(const StageArgs& a, int smemLimit, TmaPlan& pl, int ma
     if (a.fld[0]) pl.oX[0] = put(4 * P * 8);
     if (a.fld[1]) pl.oX[1] = put(2 * PP * 8);
     pl.oVelOwn = put(8 * P * (int)sizeof(R));
-    pl.oVelNbr = put(8 * P * (int)sizeof(R));
   } else {
     if (a.fld[0]) pl.oX[0] = put(2 * PP * 8);
     if (a.fld[1]) pl.oX[1] = put(PP * 8);

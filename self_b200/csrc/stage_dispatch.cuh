@@ -27,9 +27,8 @@ template <int P, class Phys, typename R>
 cudaError_t launch_one(const StageArgs& a, const StageLaunch& L, cudaStream_t st, int* usedTma) {
   *usedTma = 0;
   if constexpr (P % 2 == 0) {
-    bool ok = L.allowTma && a.mode != MODE_TRACES && aligned16(a.q) && aligned16(a.G) && aligned16(a.dsdx) &&
-              aligned16(a.J) && aligned16(a.nHat) && aligned16(a.nScale) && aligned16(a.sideInfo) &&
-              aligned16(a.trIn) && (a.velIn == nullptr || aligned16(a.velIn));
+    bool ok = L.allowTma && a.mode != MODE_TRACES && a.geo != nullptr && aligned16(a.geo) && aligned16(a.q) &&
+              aligned16(a.G) && aligned16(a.trIn) && (a.velIn == nullptr || aligned16(a.velIn));
     for (int k = 0; k < 5; ++k) ok = ok && (a.fld[k] == nullptr || aligned16(a.fld[k]));
     TmaPlan pl{};
     if (ok && make_tma_plan<P, Phys, R>(a, L.smemOptin, pl, L.maxGroups)) {
