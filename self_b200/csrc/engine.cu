@@ -267,6 +267,7 @@ int selfgpu_model2d_set_interp(selfgpu_model2d* m, const double* dgMatrix, const
   const int P = m->P;
   std::memcpy(m->base.dgM, dgMatrix, sizeof(double) * P * P);
   std::memcpy(m->base.bM, bMatrix, sizeof(double) * 2 * P);
+  for (int k = 0; k < 2 * P; ++k) m->base.bMf[k] = (float)bMatrix[k];
   std::memcpy(m->base.qw, qWeights, sizeof(double) * P);
   m->haveInterp = true;
   m->drop_graphs();

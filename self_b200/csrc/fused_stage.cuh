@@ -80,11 +80,26 @@ struct StageArgs {
   long long waitCycles;
   int* err;
   int debugStarve;  // test hook: the producer registers the first tile but issues no copies
-  // operator matrices (Lagrange%Init): dgM(ii,i) at [ii + P*i], bM(ii,side), qw
+  // operator matrices (Lagrange%Init): dgM(ii,i) at [ii + P*i], bM(ii,side), qw;
+  // bMf holds bM rounded to float for the FP32-bulk form
   double dgM[kMaxP * kMaxP];
   double bM[2 * kMaxP];
   double qw[kMaxP];
+  float bMf[2 * kMaxP];
 };
+
+// Boundary interpolation weights of the left (S, W) and right (E, N) ends as
+// kernel-parameter constants (compile-time index m after unrolling).
+template <typename R>
+__device__ __forceinline__ R bm_left(const StageArgs& a, int m) {
+  if constexpr (sizeof(R) == 8) return a.bM[m];
+  else return a.bMf[m];
+}
+template <typename R, int P>
+__device__ __forceinline__ R bm_right(const StageArgs& a, int m) {
+  if constexpr (sizeof(R) == 8) return a.bM[m + P];
+  else return a.bMf[m + P];
+}
 
 // Doubles in one element's packed geometry record: dsdx (4 P^2), nHat (8 P),
 // nScale (4 P), J (P^2), sideInfo (20 ints = 10 doubles).

@@ -83,7 +83,7 @@ struct TmaTraits {
   static constexpr int TS = trace_side_stride<P, NT, R>();
   static constexpr int TPE = (PP + 31) / 32 * 32;
   static_assert(TPE >= 4 * P, "the face phase gives each of the 4P face nodes its own thread");
-  static constexpr int kMaxGroups = 9;
+  static constexpr int kMaxGroups = 9;  // 608 threads: 96 registers each without spills (10 groups forces 80)
   static constexpr int kThreadsMax = 32 + kMaxGroups * TPE;
   // per-group compute arrays (bulk type): the node fields of the updated
   // solution alias the contravariant flux, then the boundary-normal flux
@@ -386,12 +386,25 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     }
     named_bar(barId, TPE);
 
-    // ---- E: traces of the updated solution -> trace cache
+    // ---- E: traces of the updated solution -> trace cache.  One task per
+    // (field, line, orientation) reads the line's P values once and forms both
+    // of its end traces (BoundaryInterp, src/SELF_Lagrange.f90:2241-2270):
+    // column l gives S (side 0) and N (side 2), row l gives W (3) and E (1).
     {
       R* o = trOut + (size_t)4 * TS * e;
-      for (int kk = t; kk < 4 * NT * P; kk += TPE) {
-        const int ii = kk % P, fs = kk / P, fi = fs % NT, s1 = fs / NT;
-        o[ii + P * fi + TS * s1] = face_trace_uniform<P, R>(gU + fi * PP, sb, s1, ii);
+      for (int kk = t; kk < 2 * NT * P; kk += TPE) {
+        const int fi = kk / (2 * P), rem = kk - fi * 2 * P, row = rem / P, l = rem - row * P;
+        const R* fv = gU + fi * PP + (row ? P * l : l);
+        const int stride = row ? 1 : P;
+        R lo = (R)0, hi = (R)0;
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+          const R x = fv[stride * m];
+          lo = lo + bm_left<R>(a, m) * x;
+          hi = hi + bm_right<R, P>(a, m) * x;
+        }
+        o[l + P * fi + TS * (row ? 3 : 0)] = lo;
+        o[l + P * fi + TS * (row ? 1 : 2)] = hi;
       }
     }
     // no barrier here: the next element's post-wait barrier orders the reuse of gU
