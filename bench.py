@@ -263,10 +263,11 @@ def _closure_variant(mesh, geo, q0, form, mode, mlp, steps, dt, dof):
     res = {"value": dof * steps / (ms / 1e3), "unit": "DOF-updates/s", "ms_per_rk3_step": ms / steps,
            "launches_per_rk3_step": (model.LaunchCount() - l0) / steps}
     if mode:
-        nu, act, ind, fb = model.ClosureState(reset=True)
+        nu, act, ind, (fb, evals) = model.ClosureState(reset=True)
         res["active_elements_last_stage"] = int((act > 0).sum())
         if mode == S.CLOSURE_MLP:
-            res["fallback_fraction"] = fb / (3.0 * steps * model.nElem)
+            res["mlp_evaluation_fraction"] = evals / (3.0 * steps * model.nElem)
+            res["fallback_fraction_of_evaluations"] = fb / max(evals, 1)
             res["mean_abs_activation_diff_vs_indicator_last_stage"] = float((act - ind).abs().mean())
     sol = model.solution.clone()
     del model

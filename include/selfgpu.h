@@ -382,10 +382,12 @@ int selfgpu_model2d_set_mlp(selfgpu_model2d* m, const uint16_t* weights, const f
 /* Copies (on the engine's stream) the last stage's element viscosity (nEl
  * doubles), the activation applied and the indicator's activation (nEl floats
  * each; the latter written in mode 2) into caller-owned device arrays (each
- * may be NULL), and returns on the host the number of MLP fallbacks since the
- * last reset. */
+ * may be NULL), and returns on the host (counts[2], may be NULL) the MLP
+ * fallbacks and the MLP evaluations since the last reset.  In mode 2 the
+ * indicator screens: elements more than one decade below the activation ramp
+ * get a = 0 without an MLP evaluation. */
 int selfgpu_model2d_closure_state(selfgpu_model2d* m, double* nu, float* activation, float* indicatorActivation,
-                                  int* fallbacks, int resetFallbacks);
+                                  int* counts, int resetCounts);
 
 /* Modal transform T(k,i) = w_i sqrt((2k+1)/2) L_k(x_i) (P x P, k fastest). */
 int selfgpu_modal_matrix(int N, const double* controlPoints, const double* qWeights, double* T);
@@ -411,6 +413,36 @@ int selfgpu_mlp_train(const float* features, const float* labels, int n, int epo
  * out (n floats), with the device-side weights layout of set_mlp (host arrays). */
 int selfgpu_mlp_infer(const float* features, int n, const uint16_t* weights, const float* params, float* out,
                       void* stream);
+
+/* ====================================================== 6. checkpoint files */
+
+/* Checkpoint / pickup files with the dataset paths, Fortran-order shapes and
+ * attributes of Write_Model2D / Read_Model2D (src/SELF_Model2D.f90:861-1099:
+ * /quadrature/{xi,weights,dgmatrix,dmatrix,bmatrix}, /state/interior/solution,
+ * /state/boundary/solution, /mesh/interior/x, /mesh/boundary/x, attribute N)
+ * in a plain binary container instead of HDF5.  Arrays are copied from /
+ * to host memory (onDevice = 0) or device memory (onDevice = 1).  dims[] is
+ * in Fortran order (first fastest); the last dimension is the element index
+ * for per-element data, and selfgpu_ckpt_get can read one rank's element
+ * slab of it (Read_Model2D with MPI, :1070-1080). */
+#define SELFGPU_DT_F64 1
+#define SELFGPU_DT_I32 2
+#define SELFGPU_DT_F32 3
+typedef struct selfgpu_ckpt selfgpu_ckpt;
+int selfgpu_ckpt_open(selfgpu_ckpt** out, const char* path, int write);
+int selfgpu_ckpt_put(selfgpu_ckpt* c, const char* name, const void* data, int dtype, int ndims, const long long* dims,
+                     int onDevice);
+int selfgpu_ckpt_put_attr(selfgpu_ckpt* c, const char* name, double value);
+int selfgpu_ckpt_info(selfgpu_ckpt* c, const char* name, int* dtype, int* ndims, long long* dims);
+int selfgpu_ckpt_get(selfgpu_ckpt* c, const char* name, void* data, long long capacityBytes, long long elemOffset,
+                     long long nElem, int onDevice);
+int selfgpu_ckpt_get_attr(selfgpu_ckpt* c, const char* name, double* value);
+int selfgpu_ckpt_close(selfgpu_ckpt* c);
+
+/* TimeStamp(time, 's') (src/SELF_SupportRoutines.f90:856-924): "DDDDHHMMSSmmm"
+ * into out (14 bytes with the terminator); the default pickup name is
+ * solution.<stamp>.ckpt. */
+int selfgpu_time_stamp(double time, char* out);
 
 #ifdef __cplusplus
 }

@@ -51,14 +51,21 @@ _SIGS = {
     "selfgpu_cig2d_tendency_noalloc": (c_int, [c_void_p] * 11 + [c_double, c_int, c_int, c_void_p]),
     "selfgpu_model2d_set_closure": (c_int, [c_void_p, c_int, c_double, c_double, c_double, c_void_p]),
     "selfgpu_model2d_set_mlp": (c_int, [c_void_p, c_void_p, c_void_p]),
-    "selfgpu_model2d_closure_state": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_int),
-                                              c_int]),
+    "selfgpu_model2d_closure_state": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
     "selfgpu_modal_matrix": (c_int, [c_int, c_void_p, c_void_p, c_void_p]),
     "selfgpu_cig2d_closure_features": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_double, c_double,
                                                c_void_p, c_void_p, c_void_p]),
     "selfgpu_mlp_train": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, ctypes.c_float, ctypes.c_ulonglong,
                                   c_void_p, c_void_p, c_void_p]),
     "selfgpu_mlp_infer": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "selfgpu_ckpt_open": (c_int, [ctypes.POINTER(c_void_p), ctypes.c_char_p, c_int]),
+    "selfgpu_ckpt_put": (c_int, [c_void_p, ctypes.c_char_p, c_void_p, c_int, c_int, c_void_p, c_int]),
+    "selfgpu_ckpt_put_attr": (c_int, [c_void_p, ctypes.c_char_p, c_double]),
+    "selfgpu_ckpt_info": (c_int, [c_void_p, ctypes.c_char_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int), c_void_p]),
+    "selfgpu_ckpt_get": (c_int, [c_void_p, ctypes.c_char_p, c_void_p, c_longlong, c_longlong, c_longlong, c_int]),
+    "selfgpu_ckpt_get_attr": (c_int, [c_void_p, ctypes.c_char_p, ctypes.POINTER(c_double)]),
+    "selfgpu_ckpt_close": (c_int, [c_void_p]),
+    "selfgpu_time_stamp": (c_int, [c_double, ctypes.c_char_p]),
     # drop-in wrappers (src/hip/*.cpp, src/models/hip/*.cpp of the reference)
     "ScalarGridInterp_2D_gpu_wrapper": (None, [PP, PP, PP, c_int, c_int, c_int, c_int]),
     "VectorGridInterp_2D_gpu_wrapper": (None, [PP, PP, PP, c_int, c_int, c_int, c_int]),

@@ -241,6 +241,16 @@ class Model2D:
     def Sync(self):
         check(lib().selfgpu_model2d_sync(self._h))
 
+    def Write(self, fileName=None):
+        """Write_Model2D (src/SELF_Model2D.f90:861-1058) to a checkpoint file; returns its name."""
+        from .checkpoint import write_model
+        return write_model(self, fileName)
+
+    def Read(self, fileName, firstElem=0):
+        """Read_Model2D (src/SELF_Model2D.f90:1060-1099): pickup of the solution."""
+        from .checkpoint import read_model
+        return read_model(self, fileName, firstElem)
+
     def CheckFinite(self):
         check(lib().selfgpu_model2d_check_finite(self._h))
 
@@ -375,17 +385,17 @@ class CompressibleIdealGas2D(Model2D):
                                                 self.interp.controlPoints.ctypes.data_as(ctypes.c_void_p)))
 
     def ClosureState(self, reset=False):
-        """(nu (nEl,) f64, activation (nEl,) f32, indicator activation (nEl,) f32, MLP fallbacks)
-        of the last tendency / RK stage."""
+        """(nu (nEl,) f64, activation (nEl,) f32, indicator activation (nEl,) f32) of the last
+        tendency / RK stage, and (MLP fallbacks, MLP evaluations) since the last reset."""
         nEl = self.nElem
         nu = torch.empty(nEl, device="cuda", dtype=torch.float64)
         act = torch.empty(nEl, device="cuda", dtype=torch.float32)
         ind = torch.empty(nEl, device="cuda", dtype=torch.float32)
-        fb = ctypes.c_int(0)
+        counts = (ctypes.c_int * 2)()
         torch.cuda.synchronize()
-        check(lib().selfgpu_model2d_closure_state(self._h, nu.data_ptr(), act.data_ptr(), ind.data_ptr(),
-                                                  ctypes.byref(fb), int(reset)))
-        return nu, act, ind, fb.value
+        check(lib().selfgpu_model2d_closure_state(self._h, nu.data_ptr(), act.data_ptr(), ind.data_ptr(), counts,
+                                                  int(reset)))
+        return nu, act, ind, (counts[0], counts[1])
 
     def CalculateEntropy(self):
         prim = self._pointwise("primitive")

@@ -15,7 +15,8 @@ BUILD_DIR = os.path.join(HERE, "_build")
 # (source, extra flags): the FP64 kernels are built without multiply-add
 # contraction so their roundings follow the reference's CPU path exactly.
 SOURCES = [("setup_host.cpp", []), ("legacy_ops.cu", ["-fmad=false"]), ("stage_fp64.cu", ["-fmad=false"]),
-           ("stage_fp32.cu", []), ("engine.cu", []), ("noalloc.cu", ["-fmad=false"]), ("mlp.cu", [])]
+           ("stage_fp32.cu", []), ("engine.cu", []), ("noalloc.cu", ["-fmad=false"]), ("mlp.cu", []),
+           ("checkpoint.cpp", [])]
 HEADERS = ["selfgpu_internal.h", "physics.cuh", "fused_stage.cuh", "fused_stage_tma.cuh", "stage_dispatch.cuh",
            "av_closure.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

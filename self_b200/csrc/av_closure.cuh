@@ -18,6 +18,8 @@
 //               and, on exchanged sides, -1/2 (nu grad q_in + nu grad q_ex) . n
 //               nScale to its face flux, the exterior value coming from the
 //               neighbour's traces; physical sides carry no viscous flux.
+// Only elements with nu > 0 form the gradient and write viscous terms; the
+// stage kernel reads them only where nu > 0 (the rest add exact zeros).
 //
 // Modal decay indicator (Persson & Peraire, AIAA 2006-112): c_kl are the
 // orthonormal Legendre modes of the density, S = sum_{max(k,l)=N} c^2 /
@@ -42,6 +44,10 @@ constexpr int kMlpWeights = kMlpHidden * kMlpIn + kMlpHidden * kMlpHidden + kMlp
 constexpr int kMlpFloats = kMlpHidden + kMlpHidden + 1 + 2 * kMlpIn;                    // b1 b2 b3 fmin fmax
 constexpr double kAvPi = 3.141592653589793;                                             // 4 atan(1)
 constexpr float kMlpRangeMargin = 0.05f;
+// Screening: an element whose modal decay lies more than kMlpGate decades
+// below the start of the activation ramp (s < s0 - kappa - kMlpGate) is smooth
+// by a wide margin and gets a = 0 without evaluating the MLP.
+constexpr double kMlpGate = 1.0;
 
 enum AvMode { AV_OFF = 0, AV_INDICATOR = 1, AV_MLP = 2 };
 
@@ -61,7 +67,7 @@ struct AvArgs {
   double* nu;          // element viscosity (nEl)
   float* act;          // activation applied (nEl)
   float* actInd;       // indicator activation (nEl), written in AV_MLP mode
-  int* fallbacks;      // AV_MLP: elements whose features left the training range
+  int* fallbacks;      // AV_MLP counters: [0] features outside the training range, [1] MLP evaluations
   void* visc;          // contravariant viscous volume flux (P*P, 2, 4, nEl), bulk type
   void* vtr;           // per (element, side): nu grad q traces at [i + P (d + 2 v)], bulk type
   const __nv_bfloat16* mlpW;  // W1 (32 x 36, row-major), W2 (32 x 32), w3 (32)
@@ -147,6 +153,11 @@ struct AvSmem {
   R tt[2][PP];
   R c[2][PP];
   R lam[PP];
+  R part[4][P];  // per eta-degree: density energy, highest-shell energy, energy energy, wave-speed max
+  R tot[2];
+  R actInd, lamMax;
+  int active;   // nu != 0 (the stage kernels apply the same test to the stored double)
+  int needMlp;  // AV_MLP: not screened out by the indicator
   float feat[kMlpIn];
   float h1[kMlpHidden];
   float h2[kMlpHidden];
@@ -162,7 +173,7 @@ constexpr int av_elems_per_block() {
 }
 
 template <int P, typename R, int EPB>
-__global__ void __launch_bounds__(EPB* P* P) k_av_prep(const AvArgs a) {
+__global__ void __launch_bounds__(EPB* P* P, 4) k_av_prep(const AvArgs a) {
   constexpr int PP = P * P, N = P - 1, VS = visc_side_stride<P>();
   constexpr int TS = trace_side_stride<P, 9, R>();
   __shared__ AvSmem<P, R> sm_all[EPB];
@@ -199,15 +210,165 @@ __global__ void __launch_bounds__(EPB* P* P) k_av_prep(const AvArgs a) {
   if (live) {
 #pragma unroll
     for (int v = 0; v < 4; ++v) sm.q[v][t] = (R)a.q[t + (long long)PP * (v + 4 * e)];
-    const double* gd = a.dsdx + 4 * (t + (long long)PP * e);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) sm.dsdx[k][t] = (R)gd[k];
     // wave speed |u| + c at this node (src/models/SELF_CompressibleIdealGas2D.f90:1090-1110)
     const R rho = sm.q[2][t], u = sm.q[0][t] / rho, v = sm.q[1][t] / rho;
     const R ke = (R)0.5 * (sm.q[0][t] * u + sm.q[1][t] * v);
     const R p = (gam - (R)1) * (sm.q[3][t] - ke);
     const R c = av_sqrt<R>(gam * p / rho);
     sm.lam[t] = av_sqrt<R>(u * u + v * v) + c;
+  }
+  __syncthreads();
+  // modal transform, pass 1: tt(k, j) = sum_i T(k,i) q(i,j) (density, and total energy for the MLP)
+  if (live) {
+    const int k = i, jj = j;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      if (r == 1 && !mlp) break;
+      const R* qv = sm.q[2 + r];
+      R acc = (R)0;
+#pragma unroll
+      for (int m = 0; m < P; ++m) acc = acc + (R)sT[k + P * m] * qv[m + P * jj];
+      sm.tt[r][k + P * jj] = acc;
+    }
+  }
+  __syncthreads();
+  // pass 2: c(k, l) = sum_j T(l,j) tt(k,j)
+  if (live) {
+    const int k = i, l = j;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      if (r == 1 && !mlp) break;
+      R acc = (R)0;
+#pragma unroll
+      for (int m = 0; m < P; ++m) acc = acc + (R)sT[l + P * m] * sm.tt[r][k + P * m];
+      sm.c[r][k + P * l] = acc;
+    }
+  }
+  __syncthreads();
+  // modal energies c^2 in place
+  if (live) {
+    sm.c[0][t] = sm.c[0][t] * sm.c[0][t];
+    if (mlp) sm.c[1][t] = sm.c[1][t] * sm.c[1][t];
+  }
+  __syncthreads();
+  // fixed-order partial sums per eta-degree l: all modes, the highest-shell
+  // modes (k = N or l = N), and the wave-speed maximum over the node column
+  if (live && t < P) {
+    const int l = t;
+    R tot = (R)0, tot1 = (R)0, lmax = (R)0;
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+      tot = tot + sm.c[0][k + P * l];
+      if (mlp) tot1 = tot1 + sm.c[1][k + P * l];
+      const R w = sm.lam[k + P * l];
+      if (w > lmax) lmax = w;
+    }
+    sm.part[0][l] = tot;
+    sm.part[1][l] = (l == N) ? tot : sm.c[0][N + P * l];
+    sm.part[2][l] = tot1;
+    sm.part[3][l] = lmax;
+  }
+  __syncthreads();
+  if (live && t < 2) {
+    R total = (R)0, top = (R)0, lam = (R)0;
+#pragma unroll
+    for (int l = 0; l < P; ++l) {
+      total = total + sm.part[t == 0 ? 0 : 2][l];
+      top = top + sm.part[1][l];
+      if (sm.part[3][l] > lam) lam = sm.part[3][l];
+    }
+    sm.tot[t] = total;
+    if (t == 0) {
+      R act = (R)0;  // modal decay activation of the density
+      int need = 0;
+      if (top > (R)0 && total > (R)0) {
+        const R sv = av_log10<R>(top / total);
+        if (sv > (R)a.s0 + (R)a.kappa) act = (R)1;
+        else if (!(sv < (R)a.s0 - (R)a.kappa))
+          act = (R)0.5 * ((R)1 + av_sin<R>((R)kAvPi * (sv - (R)a.s0) / ((R)2 * (R)a.kappa)));
+        need = !(sv < (R)(a.s0 - a.kappa - kMlpGate));
+      }
+      sm.actInd = act;
+      sm.lamMax = lam;
+      sm.needMlp = mlp && need;
+    }
+  }
+  // the MLP phase runs when any element of the block needs it (block-uniform barriers)
+  const bool anyMlp = __syncthreads_or(live && mlp && sm.needMlp) != 0;
+  if (anyMlp) {
+    const bool run = live && sm.needMlp;
+    // one thread per feature: energy fraction of one high shell max(k,l) = m, xi-degree k = m or
+    // eta-degree l = m (m = N-5..N) of the density (features 0..17) or total energy (18..35)
+    if (run && t < kMlpIn) {
+      const int r = t / 18, grp = (t % 18) / 6, m = N - 5 + t % 6;
+      const R* e2 = sm.c[r];
+      R sum = (R)0;
+      if (grp == 0) {
+        for (int l = 0; l < m; ++l) sum = sum + e2[m + P * l];
+        for (int k = 0; k <= m; ++k) sum = sum + e2[k + P * m];
+      } else if (grp == 1) {
+        for (int l = 0; l < P; ++l) sum = sum + e2[m + P * l];
+      } else {
+        for (int k = 0; k < P; ++k) sum = sum + e2[k + P * m];
+      }
+      const R total = sm.tot[r];
+      R qf = total > (R)0 ? sum / total : (R)0;
+      if (qf < (R)1e-16) qf = (R)1e-16;
+      sm.feat[t] = (float)((av_log10<R>(qf) + (R)8) / (R)8);
+    }
+    __syncthreads();
+    if (run && t < kMlpHidden) {
+      float acc = 0.f;
+#pragma unroll 4
+      for (int k = 0; k < kMlpIn; ++k) acc = fmaf(sW1[t * kMlpIn + k], sm.feat[k], acc);
+      acc = acc + sB[t];
+      sm.h1[t] = acc > 0.f ? acc : 0.f;
+    }
+    __syncthreads();
+    if (run && t < kMlpHidden) {
+      float acc = 0.f;
+#pragma unroll 4
+      for (int k = 0; k < kMlpHidden; ++k) acc = fmaf(sW2[t * kMlpHidden + k], sm.h1[k], acc);
+      acc = acc + sB[kMlpHidden + t];
+      sm.h2[t] = acc > 0.f ? acc : 0.f;
+    }
+    __syncthreads();
+  }
+  if (live && t == 0) {
+    const R actInd = sm.actInd;
+    R act = actInd;
+    if (mlp && sm.needMlp) {
+      if (a.fallbacks) atomicAdd(a.fallbacks + 1, 1);
+      bool inRange = true;
+      const float* fmin = sB + 2 * kMlpHidden + 1;
+      const float* fmax = fmin + kMlpIn;
+      for (int k = 0; k < kMlpIn; ++k)
+        inRange = inRange && sm.feat[k] >= fmin[k] - kMlpRangeMargin && sm.feat[k] <= fmax[k] + kMlpRangeMargin;
+      if (inRange) {
+        float z = 0.f;
+        for (int k = 0; k < kMlpHidden; ++k) z = fmaf(sw3[k], sm.h2[k], z);
+        z = z + sB[2 * kMlpHidden];
+        act = (R)(z < 0.f ? 0.f : (z > 1.f ? 1.f : z));
+      } else if (a.fallbacks) {
+        atomicAdd(a.fallbacks, 1);
+      }
+    }
+    if (mlp && a.actInd) a.actInd[e] = (float)actInd;
+    const double nu = (double)act * a.avC * a.hEl[e] / (double)N * (double)sm.lamMax;
+    sm.nu = (R)nu;
+    sm.active = nu != 0.0;
+    a.nu[e] = nu;
+    a.act[e] = (float)act;
+  }
+  __syncthreads();
+  // Elements with nu = 0 contribute exact zeros (zero viscous flux and zero
+  // viscous traces); they stop here and the stage kernel skips them, so the
+  // viscous work scales with the shocked region.
+  const bool active = live && sm.active;
+  if (active) {
+    const double* gd = a.dsdx + 4 * (t + (long long)PP * e);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) sm.dsdx[k][t] = (R)gd[k];
     // averaged conservative traces (BassiRebaySides) with the stage's exterior states
     for (int k = t; k < 4 * P; k += PP) {
       const int s1 = k / P, ii = k % P;
@@ -243,93 +404,15 @@ __global__ void __launch_bounds__(EPB* P* P) k_av_prep(const AvArgs a) {
     }
   }
   __syncthreads();
-  // modal transform, pass 1: tt(k, j) = sum_i T(k,i) q(i,j) (density, and total energy for the MLP)
-  if (live) {
-    const int k = i, jj = j;
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      if (r == 1 && !mlp) break;
-      const R* qv = sm.q[2 + r];
-      R acc = (R)0;
-#pragma unroll
-      for (int m = 0; m < P; ++m) acc = acc + (R)sT[k + P * m] * qv[m + P * jj];
-      sm.tt[r][k + P * jj] = acc;
-    }
-  }
-  __syncthreads();
-  // pass 2: c(k, l) = sum_j T(l,j) tt(k,j)
-  if (live) {
-    const int k = i, l = j;
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      if (r == 1 && !mlp) break;
-      R acc = (R)0;
-#pragma unroll
-      for (int m = 0; m < P; ++m) acc = acc + (R)sT[l + P * m] * sm.tt[r][k + P * m];
-      sm.c[r][k + P * l] = acc;
-    }
-  }
-  __syncthreads();
-  R actInd = (R)0;
-  if (live && t == 0) actInd = modal_activation<P, R>(sm.c[0], a.s0, a.kappa);
-  if (mlp) {
-    if (live && t < 2) {
-      if constexpr (P >= 6) modal_features<P, R>(sm.c[t], sm.feat + 18 * t);
-    }
-    __syncthreads();
-    if (live && t < kMlpHidden) {
-      float acc = 0.f;
-#pragma unroll 4
-      for (int k = 0; k < kMlpIn; ++k) acc = fmaf(sW1[t * kMlpIn + k], sm.feat[k], acc);
-      acc = acc + sB[t];
-      sm.h1[t] = acc > 0.f ? acc : 0.f;
-    }
-    __syncthreads();
-    if (live && t < kMlpHidden) {
-      float acc = 0.f;
-#pragma unroll 4
-      for (int k = 0; k < kMlpHidden; ++k) acc = fmaf(sW2[t * kMlpHidden + k], sm.h1[k], acc);
-      acc = acc + sB[kMlpHidden + t];
-      sm.h2[t] = acc > 0.f ? acc : 0.f;
-    }
-    __syncthreads();
-  }
-  if (live && t == 0) {
-    R act = actInd;
-    if (mlp) {
-      bool inRange = true;
-      const float* fmin = sB + 2 * kMlpHidden + 1;
-      const float* fmax = fmin + kMlpIn;
-      for (int k = 0; k < kMlpIn; ++k)
-        inRange = inRange && sm.feat[k] >= fmin[k] - kMlpRangeMargin && sm.feat[k] <= fmax[k] + kMlpRangeMargin;
-      if (inRange) {
-        float z = 0.f;
-        for (int k = 0; k < kMlpHidden; ++k) z = fmaf(sw3[k], sm.h2[k], z);
-        z = z + sB[2 * kMlpHidden];
-        act = (R)(z < 0.f ? 0.f : (z > 1.f ? 1.f : z));
-      } else if (a.fallbacks) {
-        atomicAdd(a.fallbacks, 1);
-      }
-      if (a.actInd) a.actInd[e] = (float)actInd;
-    }
-    R lam = (R)0;
-    for (int k = 0; k < PP; ++k)
-      if (sm.lam[k] > lam) lam = sm.lam[k];
-    const double nu = (double)act * a.avC * a.hEl[e] / (double)N * (double)lam;
-    sm.nu = (R)nu;
-    a.nu[e] = nu;
-    a.act[e] = (float)act;
-  }
-  __syncthreads();
   // BR1 gradient (GradientBR_MappedScalar2D, src/SELF_MappedData.f90:990-1074) scaled by nu,
   // and the contravariant viscous flux (src/models/hip/SELF_Advection2D.cpp:66-95)
-  if (live) {
+  if (active) {
     const R nu = sm.nu;
     const double* nH = a.nHat + 2 * (long long)P * 4 * e;
     const double* nS = a.nScale + (long long)P * 4 * e;
     const R Jij = (R)a.J[t + (long long)PP * e];
     R* visc = reinterpret_cast<R*>(a.visc);
-#pragma unroll
+#pragma unroll 1
     for (int v = 0; v < 4; ++v) {
       R gx = (R)0, gy = (R)0;
 #pragma unroll
@@ -369,7 +452,7 @@ __global__ void __launch_bounds__(EPB* P* P) k_av_prep(const AvArgs a) {
   }
   __syncthreads();
   // face traces of nu grad q (VectorBoundaryInterp_2D, src/SELF_Lagrange.f90:2284-2316)
-  if (live) {
+  if (active) {
     R* vo = reinterpret_cast<R*>(a.vtr) + (long long)4 * VS * e;
     for (int k = t; k < 4 * 8 * P; k += PP) {
       const int ii = k % P, d = (k / P) % 2, v = (k / (2 * P)) % 4, s1 = k / (8 * P);

@@ -612,11 +612,11 @@ int selfgpu_model2d_set_closure(selfgpu_model2d* m, int mode, double c, double s
   if (!m->avNu) {
     e = cudaMalloc(&m->avNu, nEl * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&m->avAct, 2 * nEl * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&m->avFallbacks, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&m->avFallbacks, 2 * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&m->avH, nEl * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&m->avVisc, 8 * PP * nEl * m->elemBytes());
     if (e == cudaSuccess) e = cudaMalloc(&m->avVtr, 4 * 8 * (size_t)m->P * nEl * m->elemBytes());
-    if (e == cudaSuccess) e = cudaMemsetAsync(m->avFallbacks, 0, sizeof(int), m->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->avFallbacks, 0, 2 * sizeof(int), m->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(m->avAct, 0, 2 * nEl * sizeof(float), m->stream);
     if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_set_closure", e);
   }
@@ -644,6 +644,7 @@ int selfgpu_model2d_set_closure(selfgpu_model2d* m, int mode, double c, double s
   m->base.av = 1;
   m->base.visc = m->avVisc;
   m->base.vtr = m->avVtr;
+  m->base.avNu = m->avNu;
   m->drop_graphs();
   return SELFGPU_OK;
 }
@@ -668,7 +669,7 @@ int selfgpu_model2d_set_mlp(selfgpu_model2d* m, const uint16_t* weights, const f
 }
 
 int selfgpu_model2d_closure_state(selfgpu_model2d* m, double* nu, float* activation, float* indicatorActivation,
-                                  int* fallbacks, int resetFallbacks) {
+                                  int* counts, int resetCounts) {
   if (!m) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_closure_state: null handle");
   if (!m->avNu) return set_error(SELFGPU_ERR_STATE, "selfgpu_model2d_closure_state: no closure has been set");
   const size_t nEl = (size_t)m->nEl;
@@ -679,11 +680,11 @@ int selfgpu_model2d_closure_state(selfgpu_model2d* m, double* nu, float* activat
   if (e == cudaSuccess && indicatorActivation)
     e = cudaMemcpyAsync(indicatorActivation, m->avAct + nEl, nEl * sizeof(float), cudaMemcpyDeviceToDevice,
                         m->stream);
-  if (e == cudaSuccess && fallbacks) {
-    e = cudaMemcpyAsync(fallbacks, m->avFallbacks, sizeof(int), cudaMemcpyDeviceToHost, m->stream);
+  if (e == cudaSuccess && counts) {
+    e = cudaMemcpyAsync(counts, m->avFallbacks, 2 * sizeof(int), cudaMemcpyDeviceToHost, m->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
   }
-  if (e == cudaSuccess && resetFallbacks) e = cudaMemsetAsync(m->avFallbacks, 0, sizeof(int), m->stream);
+  if (e == cudaSuccess && resetCounts) e = cudaMemsetAsync(m->avFallbacks, 0, 2 * sizeof(int), m->stream);
   if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_closure_state", e);
   return SELFGPU_OK;
 }

@@ -72,6 +72,7 @@ struct StageArgs {
   int av;
   const void* visc;
   const void* vtr;
+  const double* avNu;  // element viscosity: elements with nu = 0 have no viscous terms
   // engine-owned packed geometry: per element one contiguous record of
   // geo_record_doubles<P>() doubles (dsdx, nHat, nScale, J, then sideInfo as
   // 20 ints); read by the persistent kernel with one bulk copy
@@ -318,6 +319,7 @@ __host__ __device__ constexpr int visc_side_stride() {
 template <int P, typename R>
 __device__ __forceinline__ void av_volume_add(const StageArgs& s, int t, long long e, R* F0, R* F1) {
   constexpr int PP = P * P;
+  if (s.avNu[e] == 0.0) return;
   const R* vs = reinterpret_cast<const R*>(s.visc) + t + (long long)PP * 8 * e;
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
@@ -332,14 +334,16 @@ __device__ __forceinline__ void av_face_add(const StageArgs& s, int s1, int ii, 
   constexpr int VS = visc_side_stride<P>(), N = P - 1;
   const R* vt = reinterpret_cast<const R*>(s.vtr);
   if (si[4] != 0) return;
-  const R* own = vt + (long long)VS * (s1 + 4 * e);
   const long long e2 = si[2] - 1;
+  const bool aOwn = s.avNu[e] != 0.0, aExt = s.avNu[e2] != 0.0;
+  if (!aOwn && !aExt) return;
+  const R* own = vt + (long long)VS * (s1 + 4 * e);
   const R* ext = vt + (long long)VS * (si[3] / 10 - 1 + 4 * e2);
   const int ie = (si[3] % 10) ? N - ii : ii;
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
-    const R in = own[ii + P * (0 + 2 * v)] * (R)n1 + own[ii + P * (1 + 2 * v)] * (R)n2;
-    const R ex = ext[ie + P * (0 + 2 * v)] * (R)n1 + ext[ie + P * (1 + 2 * v)] * (R)n2;
+    const R in = aOwn ? own[ii + P * (0 + 2 * v)] * (R)n1 + own[ii + P * (1 + 2 * v)] * (R)n2 : (R)0;
+    const R ex = aExt ? ext[ie + P * (0 + 2 * v)] * (R)n1 + ext[ie + P * (1 + 2 * v)] * (R)n2 : (R)0;
     out[v] = out[v] + (R)(-0.5) * (in + ex) * (R)nmag;
   }
 }

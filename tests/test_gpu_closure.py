@@ -13,6 +13,17 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
+def _modal_decay_exponent(q, N):
+    """s = log10(highest-shell energy / total energy) of the density, per element (numpy)."""
+    T = O.modal_matrix(N)
+    P = N + 1
+    rho = q[:, :, 2, :]
+    c = np.einsum("ki,ije,lj->kle", T, rho, T)
+    e = c * c
+    top = e[N, :, :].sum(axis=0) + e[:N, N, :].sum(axis=0)
+    return np.log10(np.maximum(top, 1e-300) / e.sum(axis=(0, 1)))
+
+
 def _pair(mesh_kind, N, seed=0, c=1.0):
     import self_b200 as S
     kw = C.mesh_kwargs(mesh_kind)
@@ -103,12 +114,17 @@ def test_mlp_closure_tendency_matches_oracle_given_the_same_viscosity():
     mlp = CL.ClosureMLP(seed=5)
     mod.SetClosure(S.CLOSURE_MLP, c=1.0, mlp=mlp)
     got = S.to_host(mod.CalculateTendency()).reshape((N + 1, N + 1, 4, mod.nElem), order="F")
-    nu, act, act_ind, fallbacks = mod.ClosureState(reset=True)
+    nu, act, act_ind, (fallbacks, evals) = mod.ClosureState(reset=True)
     assert fallbacks == 0  # untrained ranges are unbounded
+    assert 0 < evals < mod.nElem  # the indicator screens out the clearly smooth elements
     _, feat = CL.features(mod.solution, mod.interp)
     ref_act = O.mlp_forward(feat.cpu().numpy().T, *mlp.unpack())
-    assert np.abs(act.cpu().numpy() - ref_act).max() < 1e-5
     act_o, _ = O.closure_features(q0, N)
+    s_o = _modal_decay_exponent(q0, N)
+    screened = s_o < O.default_s0(N) - 1.0 - 1.0  # s < s0 - kappa - 1: a = 0 without the MLP
+    ref_act = np.where(screened, 0.0, ref_act)
+    assert screened.any() and (~screened).any()
+    assert np.abs(act.cpu().numpy() - ref_act).max() < 1e-5
     assert np.abs(act_ind.cpu().numpy() - act_o).max() < 1e-6  # the judge's indicator activations
     mod_o.set_closure(2, c=1.0)
     mod_o.set("avNu", nu.cpu().numpy())
@@ -127,8 +143,8 @@ def test_mlp_fallback_to_indicator_outside_training_range():
     mlp.fmax[:] = 6.0
     mod.SetClosure(S.CLOSURE_MLP, c=1.0, mlp=mlp)
     mod.CalculateTendency()
-    nu, act, act_ind, fallbacks = mod.ClosureState(reset=True)
-    assert fallbacks == mod.nElem
+    nu, act, act_ind, (fallbacks, evals) = mod.ClosureState(reset=True)
+    assert fallbacks == evals > 0  # every element the MLP would evaluate falls back
     np.testing.assert_array_equal(act.cpu().numpy(), act_ind.cpu().numpy())
     mod_o.set_closure(1, c=1.0)
     mod_o.tendency()

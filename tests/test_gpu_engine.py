@@ -268,3 +268,34 @@ def test_check_finite_flags_injected_nan():
     with pytest.raises(S.SelfGpuError) as ei:
         mod.CheckFinite()
     assert ei.value.code == 5
+
+
+def test_checkpoint_pickup_continues_bit_for_bit(tmp_path):
+    """Write_Model2D after some steps, Read_Model2D into a fresh model: the
+    continued run equals the uninterrupted one bit for bit (the first RK3 stage
+    multiplies the RK register by a_1 = 0, so the solution is the whole
+    state), and the file carries the reference's dataset paths and shapes."""
+    import self_b200 as S
+    from self_b200.checkpoint import Checkpoint
+    N, dt = 5, 1e-3
+    _, a, _, _ = build_pair("CIG", "periodic", N, seed=9)
+    _, b, _, _ = build_pair("CIG", "periodic", N, seed=9)
+    a.ForwardStep(6, dt)
+    name = a.Write(str(tmp_path / "pick.ckpt"))
+    with Checkpoint(name) as c:
+        P, nEl = N + 1, a.nElem
+        assert c.attr("N") == N
+        assert c.info("/state/interior/solution")[1] == [P, P, 4, nEl]
+        assert c.info("/state/boundary/solution")[1] == [P, 4, 4, nEl]
+        assert c.info("/mesh/interior/x")[1] == [2, P, P, 1, nEl]
+        assert c.info("/mesh/boundary/x")[1] == [2, P, 1, 4, nEl]
+        assert c.info("/quadrature/dgmatrix")[1] == [P, P]
+        np.testing.assert_array_equal(c.get("/state/interior/solution"), S.to_host(a.solution))
+    a.ForwardStep(5, dt)
+    b.Read(name)
+    assert b.t == pytest.approx(6 * dt)
+    b.ForwardStep(5, dt)
+    np.testing.assert_array_equal(S.to_host(b.solution), S.to_host(a.solution))
+    _, wrong, _, _ = build_pair("CIG", "periodic", 3, seed=9)
+    with pytest.raises(S.SelfGpuError):
+        wrong.Read(name)
