@@ -444,6 +444,42 @@ int selfgpu_ckpt_close(selfgpu_ckpt* c);
  * solution.<stamp>.ckpt. */
 int selfgpu_time_stamp(double time, char* out);
 
+/* ============================================ 7. multi-rank decomposition */
+
+/* DomainDecomp (src/SELF_Mesh.f90:2159-2177): contiguous element ranges,
+ * offsetElem[d] = first element (0-based) of rank d, offsetElem[nDomains] =
+ * nElems.  ElemToRank (:2179-2215): the rank holding the 1-based elemID. */
+int selfgpu_domain_decomp(int nElems, int nDomains, int* offsetElem);
+int selfgpu_elem_to_rank(int nDomains, const int* offsetElem, int elemID, int* domain);
+
+/* Halo plan of one rank (the B200 form of MPIExchangeAsync + ApplyFlip,
+ * src/SELF_MappedData.f90:3323-3443): the rank's sideInfo (5,4,nLocal) with
+ * each off-rank neighbour renumbered to a halo element nLocal+1..nLocal+nHalo
+ * (the fused kernels then apply flips themselves), the number of shared
+ * faces per peer rank, and per face (concatenated in peer order, shared faces
+ * sorted by their lower global (element, side)) the trace-cache block this
+ * rank sends (side + 4 * element) and the halo block it receives.
+ * sendBlocks / recvBlocks: room for 4 * nLocal ints. */
+int selfgpu_halo_plan(const int* sideInfoGlobal, int nElGlobal, int nDomains, const int* offsetElem, int rank,
+                      int* sideInfoLocal, int* nHalo, int* peerCount, int* sendBlocks, int* recvBlocks);
+
+/* Engine side of a decomposed run.  set_halo (before set_geometry) sizes the
+ * trace caches for nEl + nHalo elements.  Per RK stage the host then runs:
+ * prologue (after setting the solution) or stage m, and between them the
+ * exchange: pack the send blocks of the caches the next stage reads
+ * (selfgpu_model2d_caches: face traces, and for ShallowWater the stage-lagged
+ * velocity traces), move them to the peers (NCCL send/recv or any transport),
+ * unpack into the halo blocks.  The shock closure is single-rank. */
+int selfgpu_model2d_set_halo(selfgpu_model2d* m, int nHalo);
+int selfgpu_model2d_prologue(selfgpu_model2d* m);
+int selfgpu_model2d_stage(selfgpu_model2d* m, double dt, int stage);
+int selfgpu_model2d_caches(selfgpu_model2d* m, void** traces, int* traceBlockBytes, void** velocity,
+                           int* velocityBlockBytes);
+/* packed[k] = cache block blocks[k] / cache block blocks[k] = packed[k]
+ * (device arrays; blockBytes a multiple of 4; blocks on the device). */
+int selfgpu_pack_blocks(const void* cache, const int* blocks, int n, int blockBytes, void* packed, void* stream);
+int selfgpu_unpack_blocks(const void* packed, const int* blocks, int n, int blockBytes, void* cache, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

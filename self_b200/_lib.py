@@ -66,6 +66,17 @@ _SIGS = {
     "selfgpu_ckpt_get_attr": (c_int, [c_void_p, ctypes.c_char_p, ctypes.POINTER(c_double)]),
     "selfgpu_ckpt_close": (c_int, [c_void_p]),
     "selfgpu_time_stamp": (c_int, [c_double, ctypes.c_char_p]),
+    "selfgpu_domain_decomp": (c_int, [c_int, c_int, c_void_p]),
+    "selfgpu_elem_to_rank": (c_int, [c_int, c_void_p, c_int, ctypes.POINTER(c_int)]),
+    "selfgpu_halo_plan": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, ctypes.POINTER(c_int), c_void_p,
+                                  c_void_p, c_void_p]),
+    "selfgpu_model2d_set_halo": (c_int, [c_void_p, c_int]),
+    "selfgpu_model2d_prologue": (c_int, [c_void_p]),
+    "selfgpu_model2d_stage": (c_int, [c_void_p, c_double, c_int]),
+    "selfgpu_model2d_caches": (c_int, [c_void_p, ctypes.POINTER(c_void_p), ctypes.POINTER(c_int),
+                                       ctypes.POINTER(c_void_p), ctypes.POINTER(c_int)]),
+    "selfgpu_pack_blocks": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p]),
+    "selfgpu_unpack_blocks": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p]),
     # drop-in wrappers (src/hip/*.cpp, src/models/hip/*.cpp of the reference)
     "ScalarGridInterp_2D_gpu_wrapper": (None, [PP, PP, PP, c_int, c_int, c_int, c_int]),
     "VectorGridInterp_2D_gpu_wrapper": (None, [PP, PP, PP, c_int, c_int, c_int, c_int]),

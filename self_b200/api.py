@@ -177,6 +177,9 @@ class Model2D:
         L = self.interp
         self._mats = [np.asfortranarray(L.dgMatrix), np.asfortranarray(L.bMatrix), np.asfortranarray(L.qWeights)]
         check(lib().selfgpu_model2d_set_interp(h, *[a.ctypes.data_as(ctypes.c_void_p) for a in self._mats]))
+        self.nHalo = int(getattr(mesh, "nHalo", 0))  # halo elements of a decomposed run (self_b200.decomp)
+        if self.nHalo:
+            check(lib().selfgpu_model2d_set_halo(h, self.nHalo))
         self._sideInfo_h = np.asfortranarray(mesh.sideInfo)
         check(lib().selfgpu_model2d_set_geometry(h, _ptr(geometry.dsdx), _ptr(geometry.J), _ptr(geometry.nHat),
                                                  _ptr(geometry.nScale), _ptr(mesh.sideInfo_d),

@@ -16,7 +16,7 @@ BUILD_DIR = os.path.join(HERE, "_build")
 # contraction so their roundings follow the reference's CPU path exactly.
 SOURCES = [("setup_host.cpp", []), ("legacy_ops.cu", ["-fmad=false"]), ("stage_fp64.cu", ["-fmad=false"]),
            ("stage_fp32.cu", []), ("engine.cu", []), ("noalloc.cu", ["-fmad=false"]), ("mlp.cu", []),
-           ("checkpoint.cpp", [])]
+           ("checkpoint.cpp", []), ("decomp.cpp", [])]
 HEADERS = ["selfgpu_internal.h", "physics.cuh", "fused_stage.cuh", "fused_stage_tma.cuh", "stage_dispatch.cuh",
            "av_closure.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

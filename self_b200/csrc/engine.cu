@@ -5,6 +5,7 @@
 // a captured CUDA graph.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -59,6 +60,19 @@ __global__ void k_pack_geometry(const double* __restrict__ dsdx, const double* _
   }
 }
 
+// Gather (scatter = 0) or scatter (scatter = 1) of n cache blocks of `words`
+// 32-bit words: packed[k] <-> cache[blocks[k]].
+__global__ void k_move_blocks(const uint32_t* __restrict__ src, const int* __restrict__ blocks, int n, int words,
+                              uint32_t* __restrict__ dst, int scatter) {
+  const long long total = (long long)n * words;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
+    const long long b = k / words, w = k - b * words;
+    const long long c = (long long)blocks[b] * words + w;
+    if (scatter) dst[c] = src[k];
+    else dst[k] = src[c];
+  }
+}
+
 int nt_of(int model) { return model == SELFGPU_MODEL_CIG ? 9 : 3; }
 int nv_of(int model) { return model == SELFGPU_MODEL_CIG ? 4 : 3; }
 
@@ -72,6 +86,7 @@ struct selfgpu_model2d {
   bool haveInterp = false, haveGeometry = false, haveState = false;
   void* tr[2] = {nullptr, nullptr};
   void* vel[2] = {nullptr, nullptr};
+  int nHalo = 0;   // halo elements after the rank's own in the caches (multi-rank runs)
   int cur = 0;     // index of the trace buffer holding the current solution's traces
   int vcur = 0;    // index of the velocity buffer the next stage reads (SW)
   bool valid = false;
@@ -152,23 +167,49 @@ struct selfgpu_model2d {
     return launch(a);
   }
 
+  // Issue RK stage m (0, 1, 2) from the current parities.
+  cudaError_t stage_once(double dt, int m) {
+    StageArgs a = base;
+    a.mode = MODE_RK;
+    a.rk_a = kRK3a[m];
+    a.rk_gdt = kRK3g[m] * dt;
+    a.rk_g = kRK3g[m];
+    a.trIn = tr[cur];
+    a.trOut = tr[1 - cur];
+    if (model == SELFGPU_MODEL_SW) {
+      a.velIn = vel[vcur];
+      a.velOut = vel[1 - vcur];
+      vcur = 1 - vcur;
+    }
+    cur = 1 - cur;
+    return launch(a);
+  }
+
   // Issue the three stages of one RK step starting from the current parities.
   cudaError_t step(double dt) {
     for (int m = 0; m < 3; ++m) {
-      StageArgs a = base;
-      a.mode = MODE_RK;
-      a.rk_a = kRK3a[m];
-      a.rk_gdt = kRK3g[m] * dt;
-      a.rk_g = kRK3g[m];
-      a.trIn = tr[cur];
-      a.trOut = tr[1 - cur];
-      if (model == SELFGPU_MODEL_SW) {
-        a.velIn = vel[vcur];
-        a.velOut = vel[1 - vcur];
-        vcur = 1 - vcur;
-      }
-      cur = 1 - cur;
-      cudaError_t e = launch(a);
+      cudaError_t e = stage_once(dt, m);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+
+  size_t trace_block_bytes() const {  // one (element, side) block of the trace cache
+    const size_t per16 = 16 / elemBytes();
+    return ((size_t)nt_of(model) * P + per16 - 1) / per16 * per16 * elemBytes();
+  }
+  size_t vel_block_bytes() const { return (size_t)2 * P * elemBytes(); }
+
+  cudaError_t alloc_caches() {
+    for (int k = 0; k < 2; ++k) {
+      if (tr[k]) cudaFree(tr[k]);
+      if (vel[k]) cudaFree(vel[k]);
+      tr[k] = vel[k] = nullptr;
+    }
+    const size_t nb = 4 * (size_t)(nEl + nHalo);
+    for (int k = 0; k < 2; ++k) {
+      cudaError_t e = cudaMalloc(&tr[k], trace_block_bytes() * nb);
+      if (e == cudaSuccess && model == SELFGPU_MODEL_SW) e = cudaMalloc(&vel[k], vel_block_bytes() * nb);
       if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -214,16 +255,10 @@ int selfgpu_model2d_create(selfgpu_model2d** out, int model, int N, int nEl, int
   }
   // one (element, side) block holds NT fields x P nodes, padded to 16 bytes
   // (trace_side_stride in fused_stage.cuh)
-  const size_t per16 = 16 / m->elemBytes();
-  const size_t ts = ((size_t)nt_of(model) * m->P + per16 - 1) / per16 * per16;
-  const size_t trBytes = ts * 4 * (size_t)nEl * m->elemBytes();
-  for (int k = 0; k < 2; ++k) {
-    e = cudaMalloc(&m->tr[k], trBytes);
-    if (e == cudaSuccess && model == SELFGPU_MODEL_SW) e = cudaMalloc(&m->vel[k], (size_t)m->P * 2 * 4 * nEl * m->elemBytes());
-    if (e != cudaSuccess) {
-      selfgpu_model2d_destroy(m);
-      return fail_cuda("selfgpu_model2d_create: trace cache", e);
-    }
+  e = m->alloc_caches();
+  if (e != cudaSuccess) {
+    selfgpu_model2d_destroy(m);
+    return fail_cuda("selfgpu_model2d_create: trace cache", e);
   }
   e = cudaMalloc(&m->dflag, 2 * sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(m->dflag, 0, 2 * sizeof(int));
@@ -280,7 +315,7 @@ int selfgpu_model2d_set_geometry(selfgpu_model2d* m, const double* dsdx, const d
     return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_geometry: null argument");
   if (((uintptr_t)dsdx % 16) || ((uintptr_t)nHat % 16))
     return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_geometry: dsdx and nHat must be 16-byte aligned");
-  int rc = validate_side_info(sideInfo_h, m->nEl);
+  int rc = validate_side_info(sideInfo_h, m->nEl, m->nEl + m->nHalo);
   if (rc != SELFGPU_OK) return rc;
   m->base.dsdx = dsdx;
   m->base.J = J;
@@ -598,6 +633,9 @@ int selfgpu_model2d_set_closure(selfgpu_model2d* m, int mode, double c, double s
   }
   if (m->model != SELFGPU_MODEL_CIG)
     return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_closure: the closure is defined for CompressibleIdealGas2D");
+  if (m->nHalo > 0)
+    return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_closure: the closure is single-rank (no halo exchange of "
+                                      "viscous terms)");
   if (mode != AV_INDICATOR && mode != AV_MLP)
     return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_closure: unknown closure mode");
   if (mode == AV_MLP && (m->P < 6 || !m->mlpW))
@@ -701,6 +739,76 @@ int selfgpu_cig2d_closure_features(const double* q, int N, int nEl, const double
   modal_matrix(N, controlPoints, qWeights, x.T);
   cudaError_t e = launch_closure_features(q, N + 1, nEl, x, activation, features, (cudaStream_t)stream);
   if (e != cudaSuccess) return fail_cuda("selfgpu_cig2d_closure_features", e);
+  return SELFGPU_OK;
+}
+
+int selfgpu_model2d_set_halo(selfgpu_model2d* m, int nHalo) {
+  if (!m || nHalo < 0) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_halo: bad arguments");
+  if (m->avMode != AV_OFF)
+    return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_halo: the closure is single-rank");
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  m->drop_graphs();
+  m->nHalo = nHalo;
+  cudaError_t e = m->alloc_caches();
+  if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_set_halo", e);
+  m->haveGeometry = false;  // sideInfo is validated against the new neighbour range
+  m->valid = false;
+  return SELFGPU_OK;
+}
+
+int selfgpu_model2d_prologue(selfgpu_model2d* m) {
+  int rc = check_ready(m, "selfgpu_model2d_prologue");
+  if (rc) return rc;
+  cudaError_t e = m->prologue();
+  if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_prologue", e);
+  return SELFGPU_OK;
+}
+
+int selfgpu_model2d_stage(selfgpu_model2d* m, double dt, int stage) {
+  int rc = check_ready(m, "selfgpu_model2d_stage");
+  if (rc) return rc;
+  if (stage < 0 || stage > 2) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_stage: stage must be 0, 1 or 2");
+  if (!m->valid)
+    return set_error(SELFGPU_ERR_STATE, "selfgpu_model2d_stage: the trace caches are stale (call "
+                                        "selfgpu_model2d_prologue after setting the solution)");
+  cudaError_t e = m->stage_once(dt, stage);
+  if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_stage", e);
+  return SELFGPU_OK;
+}
+
+int selfgpu_model2d_caches(selfgpu_model2d* m, void** traces, int* traceBlockBytes, void** velocity,
+                           int* velocityBlockBytes) {
+  if (!m) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_caches: null handle");
+  if (traces) *traces = m->tr[m->cur];
+  if (traceBlockBytes) *traceBlockBytes = (int)m->trace_block_bytes();
+  if (velocity) *velocity = (m->model == SELFGPU_MODEL_SW) ? m->vel[m->vcur] : nullptr;
+  if (velocityBlockBytes) *velocityBlockBytes = (m->model == SELFGPU_MODEL_SW) ? (int)m->vel_block_bytes() : 0;
+  return SELFGPU_OK;
+}
+
+int selfgpu_pack_blocks(const void* cache, const int* blocks, int n, int blockBytes, void* out, void* stream) {
+  if (!cache || !blocks || n < 0 || blockBytes < 4 || blockBytes % 4 || !out)
+    return set_error(SELFGPU_ERR_ARG, "selfgpu_pack_blocks: bad arguments");
+  if (n == 0) return SELFGPU_OK;
+  const int words = blockBytes / 4;
+  const long long total = (long long)n * words;
+  k_move_blocks<<<(int)std::min<long long>((total + 255) / 256, 4096), 256, 0, (cudaStream_t)stream>>>(
+      (const uint32_t*)cache, blocks, n, words, (uint32_t*)out, 0);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail_cuda("selfgpu_pack_blocks", e);
+  return SELFGPU_OK;
+}
+
+int selfgpu_unpack_blocks(const void* packed, const int* blocks, int n, int blockBytes, void* cache, void* stream) {
+  if (!cache || !blocks || n < 0 || blockBytes < 4 || blockBytes % 4 || !packed)
+    return set_error(SELFGPU_ERR_ARG, "selfgpu_unpack_blocks: bad arguments");
+  if (n == 0) return SELFGPU_OK;
+  const int words = blockBytes / 4;
+  const long long total = (long long)n * words;
+  k_move_blocks<<<(int)std::min<long long>((total + 255) / 256, 4096), 256, 0, (cudaStream_t)stream>>>(
+      (const uint32_t*)packed, blocks, n, words, (uint32_t*)cache, 1);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail_cuda("selfgpu_unpack_blocks", e);
   return SELFGPU_OK;
 }
 

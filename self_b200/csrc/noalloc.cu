@@ -105,7 +105,7 @@ extern "C" int selfgpu_cig2d_tendency_noalloc(const double* solution, double* dS
                          " elements at this degree)");
   if (((uintptr_t)dsdx % 16) || ((uintptr_t)nHat % 16))
     return set_error(SELFGPU_ERR_ARG, "selfgpu_cig2d_tendency_noalloc: dsdx and nHat must be 16-byte aligned");
-  int rc = validate_side_info(sideInfo_h, nEl);
+  int rc = validate_side_info(sideInfo_h, nEl, nEl);
   if (rc != SELFGPU_OK) return rc;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);

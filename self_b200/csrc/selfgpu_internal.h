@@ -20,7 +20,8 @@ int lagrange_init(int N, int ctrlType, int M, int tgtType, double* ctrl, double*
 int mesh2d_structured(int nx, int ny, double x0, double x1, double y0, double y1, int perX, int perY,
                       double amp, int bcid, const int* rot, double* nodeCoords, int* globalNodeIDs,
                       int* sideInfo);
-int validate_side_info(const int* sideInfo, int nEl);
+// Neighbour ids may reach nNeighbours (= nEl, or nEl + halo elements).
+int validate_side_info(const int* sideInfo, int nEl, int nNeighbours);
 // T(k,i) = w_i sqrt((2k+1)/2) L_k(x_i): nodal -> orthonormal Legendre modes
 void modal_matrix(int N, const double* x, const double* w, double* T);
 

@@ -309,16 +309,16 @@ int mesh2d_structured(int nx, int ny, double x0, double x1, double y0, double y1
   return SELFGPU_OK;
 }
 
-int validate_side_info(const int* sideInfo, int nEl) {
+int validate_side_info(const int* sideInfo, int nEl, int nNeighbours) {
   for (int e = 0; e < nEl; ++e)
     for (int s = 0; s < 4; ++s) {
       const int* si = sideInfo + 5 * (s + 4 * (size_t)e);
       const int e2 = si[2], s2 = si[3] / 10, flip = si[3] % 10, bcid = si[4];
       if (bcid == 0) {
-        if (e2 < 1 || e2 > nEl || s2 < 1 || s2 > 4 || (flip != 0 && flip != 1))
+        if (e2 < 1 || e2 > nNeighbours || s2 < 1 || s2 > 4 || (flip != 0 && flip != 1))
           return set_error(SELFGPU_ERR_MESH, "sideInfo: element " + std::to_string(e + 1) + " side " +
                                                  std::to_string(s + 1) + " has an invalid neighbour record");
-      } else if (e2 < 0 || e2 > nEl) {
+      } else if (e2 < 0 || e2 > nNeighbours) {
         return set_error(SELFGPU_ERR_MESH, "sideInfo: element " + std::to_string(e + 1) + " side " +
                                                std::to_string(s + 1) + " has an out-of-range neighbour id");
       }
@@ -375,7 +375,7 @@ int selfgpu_modal_matrix(int N, const double* controlPoints, const double* qWeig
 
 int selfgpu_validate_side_info(const int* sideInfo, int nEl) {
   if (!sideInfo || nEl < 1) return selfgpu::set_error(SELFGPU_ERR_ARG, "selfgpu_validate_side_info: bad arguments");
-  return selfgpu::validate_side_info(sideInfo, nEl);
+  return selfgpu::validate_side_info(sideInfo, nEl, nEl);
 }
 
 }  // extern "C"
