@@ -311,9 +311,10 @@ int selfgpu_model2d_set_launch(selfgpu_model2d* m, int persistent, int groups);
 
 /* Autotuner: times the per-element-group kernel and the persistent kernel at
  * every consumer-group count that fits (elements in flight per CTA, each with
- * its double-buffered staging tile) on tendency launches over this handle's
- * own data, keeps the fastest, and reports it (persistent 0/1, group count,
- * microseconds per stage).  Allocates a temporary dSdt buffer. */
+ * its double-buffered staging tile) on RK-stage launches over this handle's
+ * own data (a zero step on scratch copies of the solution and RK register;
+ * the state is not modified), keeps the fastest, and reports it (persistent
+ * 0/1, group count, microseconds per stage).  Allocates scratch memory. */
 int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, float* usPerStage);
 
 /* Failure detection.  Every wait inside the persistent kernel is bounded; a

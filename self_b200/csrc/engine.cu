@@ -546,11 +546,20 @@ int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, f
   if (rc) return rc;
   // Candidates: the per-element-group kernel and the persistent kernel with
   // every consumer-group count from 2 up to what fits.  Each is timed on
-  // tendency launches (the state is not modified) over the handle's data.
+  // RK-stage launches over scratch copies of the solution and RK register
+  // (a zero step: the state is not modified); the stage writes the trace
+  // caches the next real stage rewrites anyway.
   const size_t n = (size_t)m->P * m->P * nv_of(m->model) * m->nEl;
   double* scratch = nullptr;
-  cudaError_t e = cudaMalloc(&scratch, n * sizeof(double));
+  cudaError_t e = cudaMalloc(&scratch, 2 * n * sizeof(double));
   if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_autotune", e);
+  e = cudaMemcpyAsync(scratch, m->base.q, n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(scratch + n, m->base.G, n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);
+  if (e != cudaSuccess) {
+    cudaFree(scratch);
+    return fail_cuda("selfgpu_model2d_autotune", e);
+  }
   if (!m->valid) {
     e = m->prologue();
     if (e != cudaSuccess) {
@@ -559,13 +568,17 @@ int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, f
     }
   }
   StageArgs a = m->base;
-  a.mode = MODE_TENDENCY;
-  a.dSdt = scratch;
+  a.mode = MODE_RK;
+  a.q = scratch;
+  a.G = scratch + n;
+  a.rk_a = 0.0;
+  a.rk_gdt = 0.0;
+  a.rk_g = 0.0;
   a.trIn = m->tr[m->cur];
-  a.trOut = nullptr;
+  a.trOut = m->tr[1 - m->cur];  // rewritten by the next real stage
   if (m->model == SELFGPU_MODEL_SW) {
     a.velIn = m->vel[m->vcur];
-    a.velOut = m->vel[1 - m->vcur];  // written, not consumed: the cache parity is left unchanged
+    a.velOut = m->vel[1 - m->vcur];  // likewise; the cache parity is left unchanged
   }
   if (m->avMode != AV_OFF) {
     e = m->launch_av(a.trIn);  // the candidates then read this state's viscous terms

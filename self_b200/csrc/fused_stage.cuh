@@ -567,12 +567,24 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
     if (a.mode == MODE_TENDENCY) return;
   }
   __syncthreads();
-  // traces of the (updated) solution -> trace cache
+  // traces of the (updated) solution -> trace cache: one task per (field,
+  // line, orientation) forms both end traces of the line (column l: S and N,
+  // row l: W and E) with the bMatrix rows as kernel-parameter constants
   R* o = trOut + (long long)4 * TS * e;
   if (live)
-    for (int k = t; k < 4 * NT * P; k += PP) {
-      const int ii = k % P, fs = k / P, fi = fs % NT, s1 = fs / NT;
-      o[ii + P * fi + TS * s1] = face_trace<P, R>(sm.fld[fi], sb, s1, ii);
+    for (int k = t; k < 2 * NT * P; k += PP) {
+      const int fi = k / (2 * P), rem = k - fi * 2 * P, row = rem / P, l = rem - row * P;
+      const R* fv = sm.fld[fi] + (row ? P * l : l);
+      const int stride = row ? 1 : P;
+      R lo = (R)0, hi = (R)0;
+#pragma unroll
+      for (int m = 0; m < P; ++m) {
+        const R x = fv[stride * m];
+        lo = lo + bm_left<R>(a, m) * x;
+        hi = hi + bm_right<R, P>(a, m) * x;
+      }
+      o[l + P * fi + TS * (row ? 3 : 0)] = lo;
+      o[l + P * fi + TS * (row ? 1 : 2)] = hi;
     }
   if constexpr (Phys::kLaggedVelocity) {
     // Start of a run: the stage-lagged velocity traces equal those of this
