@@ -351,21 +351,6 @@ __device__ __forceinline__ void av_face_add(const StageArgs& s, int s1, int ii, 
 // Boundary interpolation of one traced field at face node ii of side s1
 // (src/SELF_Lagrange.f90:2241-2270): S and N run along j at fixed i, E and W
 // along i at fixed j.
-// Same sums without a branch on the side: S/N step through j (stride P) from
-// node (ii, 0), E/W through i (stride 1) from node (0, ii); S/W use the left
-// boundary row of bMatrix, E/N the right one.
-template <int P, typename R>
-__device__ __forceinline__ R face_trace_uniform(const R* fv, const double* sb, int s1, int ii) {
-  const bool sn = (s1 & 1) == 0;
-  const int base = sn ? ii : P * ii;
-  const int stride = sn ? P : 1;
-  const double* b = sb + ((s1 == 1 || s1 == 2) ? P : 0);
-  R acc = (R)0;
-#pragma unroll
-  for (int m = 0; m < P; ++m) acc = acc + (R)b[m] * fv[base + stride * m];
-  return acc;
-}
-
 template <int P, typename R>
 __device__ __forceinline__ R face_trace(const R* fv, const double* sb, int s1, int ii) {
   R acc = (R)0;
@@ -458,6 +443,9 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
           val = trIn[(flip ? N - ii : ii) + P * fi + (long long)TS * (s2 + 4 * e2)];
         }
         sm.ext[s1][fi][ii] = val;
+        // own traces of this stage's solution: the trace cache holds them (the
+        // previous launch formed them from the same values with the same sums)
+        sm.own[s1][fi][ii] = trIn[ii + P * fi + (long long)TS * (s1 + 4 * e)];
       }
       if constexpr (Phys::kLaggedVelocity) {
         const R* vIn = reinterpret_cast<const R*>(a.velIn);
@@ -480,12 +468,6 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
     }
   }
   if (a.mode != MODE_TRACES) {
-    __syncthreads();
-    if (live)
-      for (int k = t; k < 4 * NT * P; k += PP) {
-        const int ii = k % P, fs = k / P, fi = fs % NT, s1 = fs / NT;
-        sm.own[s1][fi][ii] = face_trace<P, R>(sm.fld[fi], sb, s1, ii);
-      }
     __syncthreads();
     // 4P face nodes per element; for P <= 3 there are fewer node threads (P*P)
     if (live)
