@@ -7,13 +7,14 @@
 // templates (src/models/hip/SELF_Advection2D.cpp:66-95, :140-175) -- with one
 // viscosity per element instead of one diffusivity.
 //
-// With the closure on, each RK stage is two launches:
-//   k_av_prep   per element: element viscosity nu (modal-decay indicator of the
-//               density, or the closure MLP with the indicator as fallback),
-//               the BR1 gradient of the four conservative variables from the
-//               averaged traces of the stage's trace cache, the contravariant
-//               viscous volume flux -(dsdx^T nu grad q) and the face traces of
-//               nu grad q;
+// With the closure on, each RK stage runs, before the stage kernel:
+//   k_av_nu     one warp per element: the element viscosity nu (modal-decay
+//               indicator of the density, or the closure MLP with the indicator
+//               as fallback and screen), and the list of elements with nu > 0;
+//   k_av_grad   the listed elements only: the BR1 gradient of the four
+//               conservative variables from the averaged traces of the stage's
+//               trace cache, the contravariant viscous volume flux
+//               -(dsdx^T nu grad q) and the face traces of nu grad q;
 //   the stage   kernel adds the viscous volume flux to its contravariant flux
 //               and, on exchanged sides, -1/2 (nu grad q_in + nu grad q_ex) . n
 //               nScale to its face flux, the exterior value coming from the
@@ -68,6 +69,8 @@ struct AvArgs {
   float* act;          // activation applied (nEl)
   float* actInd;       // indicator activation (nEl), written in AV_MLP mode
   int* fallbacks;      // AV_MLP counters: [0] features outside the training range, [1] MLP evaluations
+  int* activeCount;    // elements with nu > 0 in this stage (reset before the viscosity kernel)
+  int* activeList;     // their ids (nEl capacity)
   void* visc;          // contravariant viscous volume flux (P*P, 2, 4, nEl), bulk type
   void* vtr;           // per (element, side): nu grad q traces at [i + P (d + 2 v)], bulk type
   const __nv_bfloat16* mlpW;  // W1 (32 x 36, row-major), W2 (32 x 32), w3 (32)
@@ -142,322 +145,345 @@ __device__ void modal_features(const R* c, float* f) {
   }
 }
 
-// ------------------------------------------------------------ prep kernel
+// ------------------------------------------------------ viscosity kernel
+// One warp per element (warp-level synchronisation only): density modes,
+// activation and screening; the MLP only where the indicator does not screen
+// the element out; the wave speed, the viscosity and an entry in the list of
+// active elements only where the activation is not zero.
 template <int P, typename R>
-struct AvSmem {
+struct NuWarpSmem {
+  static constexpr int PP = P * P;
+  R q[2][PP];  // density, total energy
+  R tt[PP];
+  R c[2][PP];  // modal energies c^2
+  R part[3][P];
+  float feat[kMlpIn];
+  float h1[kMlpHidden];
+};
+
+// Orthonormal modal energies of one P x P field of this warp's element:
+// c(k,l) = sum_j T(l,j) sum_i T(k,i) q(i,j), then c^2 in place.
+template <int P, typename R>
+__device__ __forceinline__ void warp_modal_energy(const double* sT, const R* q, R* tt, R* c, int lane) {
+  constexpr int PP = P * P;
+  for (int o = lane; o < PP; o += 32) {
+    const int k = o % P, jj = o / P;
+    R acc = (R)0;
+#pragma unroll
+    for (int m = 0; m < P; ++m) acc = acc + (R)sT[k + P * m] * q[m + P * jj];
+    tt[k + P * jj] = acc;
+  }
+  __syncwarp();
+  for (int o = lane; o < PP; o += 32) {
+    const int k = o % P, l = o / P;
+    R acc = (R)0;
+#pragma unroll
+    for (int m = 0; m < P; ++m) acc = acc + (R)sT[l + P * m] * tt[k + P * m];
+    c[k + P * l] = acc * acc;
+  }
+  __syncwarp();
+}
+
+constexpr int kNuWarps = 4;
+
+template <int P, typename R>
+__global__ void __launch_bounds__(32 * kNuWarps) k_av_nu(const AvArgs a) {
+  constexpr int PP = P * P, N = P - 1;
+  __shared__ NuWarpSmem<P, R> ws[kNuWarps];
+  __shared__ double sT[PP];
+  __shared__ float sW1[kMlpHidden * kMlpIn], sW2[kMlpHidden * kMlpHidden], sw3[kMlpHidden], sB[kMlpFloats];
+  const bool mlp = (a.mode == AV_MLP) && (P >= 6);
+  for (int k = threadIdx.x; k < PP; k += blockDim.x) sT[k] = a.T[k];
+  if (mlp) {
+    for (int k = threadIdx.x; k < kMlpHidden * kMlpIn; k += blockDim.x) sW1[k] = __bfloat162float(a.mlpW[k]);
+    for (int k = threadIdx.x; k < kMlpHidden * kMlpHidden; k += blockDim.x)
+      sW2[k] = __bfloat162float(a.mlpW[kMlpHidden * kMlpIn + k]);
+    for (int k = threadIdx.x; k < kMlpHidden; k += blockDim.x)
+      sw3[k] = __bfloat162float(a.mlpW[kMlpHidden * kMlpIn + kMlpHidden * kMlpHidden + k]);
+    for (int k = threadIdx.x; k < kMlpFloats; k += blockDim.x) sB[k] = a.mlpB[k];
+  }
+  __syncthreads();
+  const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
+  NuWarpSmem<P, R>& s = ws[w];
+  const R gam = (R)a.gamma;
+  for (long long e = (long long)blockIdx.x * kNuWarps + w; e < a.nEl; e += (long long)gridDim.x * kNuWarps) {
+    for (int k = lane; k < PP; k += 32) s.q[0][k] = (R)a.q[k + (long long)PP * (2 + 4 * e)];
+    __syncwarp();
+    warp_modal_energy<P, R>(sT, s.q[0], s.tt, s.c[0], lane);
+    // fixed-order sums per eta-degree l, then over l
+    if (lane < P) {
+      const int l = lane;
+      R tot = (R)0;
+#pragma unroll
+      for (int k = 0; k < P; ++k) tot = tot + s.c[0][k + P * l];
+      s.part[0][l] = tot;
+      s.part[1][l] = (l == N) ? tot : s.c[0][N + P * l];
+    }
+    __syncwarp();
+    R actInd = (R)0;
+    int need = 0;
+    if (lane == 0) {
+      R total = (R)0, top = (R)0;
+#pragma unroll
+      for (int l = 0; l < P; ++l) {
+        total = total + s.part[0][l];
+        top = top + s.part[1][l];
+      }
+      if (top > (R)0 && total > (R)0) {
+        const R sv = av_log10<R>(top / total);
+        if (sv > (R)a.s0 + (R)a.kappa) actInd = (R)1;
+        else if (!(sv < (R)a.s0 - (R)a.kappa))
+          actInd = (R)0.5 * ((R)1 + av_sin<R>((R)kAvPi * (sv - (R)a.s0) / ((R)2 * (R)a.kappa)));
+        need = mlp && !(sv < (R)(a.s0 - a.kappa - kMlpGate));
+      }
+      s.part[2][0] = total;
+    }
+    actInd = __shfl_sync(0xffffffffu, actInd, 0);
+    need = __shfl_sync(0xffffffffu, need, 0);
+    R act = actInd;
+    if (need) {
+      // the closure MLP: features of the density and total-energy modes
+      for (int k = lane; k < PP; k += 32) s.q[1][k] = (R)a.q[k + (long long)PP * (3 + 4 * e)];
+      __syncwarp();
+      warp_modal_energy<P, R>(sT, s.q[1], s.tt, s.c[1], lane);
+      if (lane < P) {
+        R tot = (R)0;
+#pragma unroll
+        for (int k = 0; k < P; ++k) tot = tot + s.c[1][k + P * lane];
+        s.part[1][lane] = tot;
+      }
+      __syncwarp();
+      if (lane == 0) {
+        R total = (R)0;
+#pragma unroll
+        for (int l = 0; l < P; ++l) total = total + s.part[1][l];
+        s.part[2][1] = total;
+      }
+      __syncwarp();
+      for (int f = lane; f < kMlpIn; f += 32) {
+        const int r = f / 18, grp = (f % 18) / 6, m = N - 5 + f % 6;
+        const R* e2 = s.c[r];
+        R sum = (R)0;
+        if (grp == 0) {
+          for (int l = 0; l < m; ++l) sum = sum + e2[m + P * l];
+          for (int k = 0; k <= m; ++k) sum = sum + e2[k + P * m];
+        } else if (grp == 1) {
+          for (int l = 0; l < P; ++l) sum = sum + e2[m + P * l];
+        } else {
+          for (int k = 0; k < P; ++k) sum = sum + e2[k + P * m];
+        }
+        const R total = s.part[2][r];
+        R qf = total > (R)0 ? sum / total : (R)0;
+        if (qf < (R)1e-16) qf = (R)1e-16;
+        s.feat[f] = (float)((av_log10<R>(qf) + (R)8) / (R)8);
+      }
+      __syncwarp();
+      {
+        float acc = 0.f;  // lane = hidden unit
+#pragma unroll 4
+        for (int k = 0; k < kMlpIn; ++k) acc = fmaf(sW1[lane * kMlpIn + k], s.feat[k], acc);
+        acc = acc + sB[lane];
+        s.h1[lane] = acc > 0.f ? acc : 0.f;
+      }
+      __syncwarp();
+      float h2;
+      {
+        float acc = 0.f;
+#pragma unroll 4
+        for (int k = 0; k < kMlpHidden; ++k) acc = fmaf(sW2[lane * kMlpHidden + k], s.h1[k], acc);
+        acc = acc + sB[kMlpHidden + lane];
+        h2 = acc > 0.f ? acc : 0.f;
+      }
+      __syncwarp();
+      s.h1[lane] = h2;  // the second hidden layer reuses the first's array
+      __syncwarp();
+      if (lane == 0) {
+        if (a.fallbacks) atomicAdd(a.fallbacks + 1, 1);
+        bool inRange = true;
+        const float* fmin = sB + 2 * kMlpHidden + 1;
+        const float* fmax = fmin + kMlpIn;
+        for (int k = 0; k < kMlpIn; ++k)
+          inRange = inRange && s.feat[k] >= fmin[k] - kMlpRangeMargin && s.feat[k] <= fmax[k] + kMlpRangeMargin;
+        if (inRange) {
+          float z = 0.f;
+          for (int k = 0; k < kMlpHidden; ++k) z = fmaf(sw3[k], s.h1[k], z);
+          z = z + sB[2 * kMlpHidden];
+          act = (R)(z < 0.f ? 0.f : (z > 1.f ? 1.f : z));
+        } else if (a.fallbacks) {
+          atomicAdd(a.fallbacks, 1);
+        }
+      }
+      act = __shfl_sync(0xffffffffu, act, 0);
+    }
+    double nu = 0.0;
+    if (act != (R)0) {
+      // wave speed |u| + c (src/models/SELF_CompressibleIdealGas2D.f90:1090-1110), max over the nodes
+      R lam = (R)0;
+      for (int k = lane; k < PP; k += 32) {
+        const long long b = k + (long long)PP * 4 * e;
+        const R ru = (R)a.q[b], rv = (R)a.q[b + PP], rho = (R)a.q[b + 2 * PP], rE = (R)a.q[b + 3 * PP];
+        const R u = ru / rho, v = rv / rho;
+        const R ke = (R)0.5 * (ru * u + rv * v);
+        const R p = (gam - (R)1) * (rE - ke);
+        const R c = av_sqrt<R>(gam * p / rho);
+        const R wv = av_sqrt<R>(u * u + v * v) + c;
+        if (wv > lam) lam = wv;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const R other = __shfl_xor_sync(0xffffffffu, lam, o);
+        if (other > lam) lam = other;
+      }
+      nu = (double)act * a.avC * a.hEl[e] / (double)N * (double)lam;
+    }
+    if (lane == 0) {
+      a.nu[e] = nu;
+      a.act[e] = (float)act;
+      if (mlp && a.actInd) a.actInd[e] = (float)actInd;
+      if (nu != 0.0) a.activeList[atomicAdd(a.activeCount, 1)] = (int)e;
+    }
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------------ viscous-term kernel
+// The active elements only (the list the viscosity kernel filled): BR1
+// gradient scaled by nu, contravariant viscous flux and face traces of nu grad q.
+template <int P, typename R>
+struct GradSmem {
   static constexpr int PP = P * P;
   R q[4][PP];
   R dsdx[4][PP];  // (dsdx11, dsdx21, dsdx12, dsdx22) per node
   R avg[4][4][P];
   R g[2][4][PP];  // nu grad q
-  R tt[2][PP];
-  R c[2][PP];
-  R lam[PP];
-  R part[4][P];  // per eta-degree: density energy, highest-shell energy, energy energy, wave-speed max
-  R tot[2];
-  R actInd, lamMax;
-  int active;   // nu != 0 (the stage kernels apply the same test to the stored double)
-  int needMlp;  // AV_MLP: not screened out by the indicator
-  float feat[kMlpIn];
-  float h1[kMlpHidden];
-  float h2[kMlpHidden];
-  R nu;
 };
 
 template <int P, typename R>
 constexpr int av_elems_per_block() {
   int e = 128 / (P * P);
   if (e < 1) e = 1;
-  while (e > 1 && (size_t)e * sizeof(AvSmem<P, R>) > 30 * 1024) --e;
+  while (e > 1 && (size_t)e * sizeof(GradSmem<P, R>) > 30 * 1024) --e;
   return e;
 }
 
 template <int P, typename R, int EPB>
-__global__ void __launch_bounds__(EPB* P* P, 4) k_av_prep(const AvArgs a) {
+__global__ void __launch_bounds__(EPB* P* P, 4) k_av_grad(const AvArgs a) {
   constexpr int PP = P * P, N = P - 1, VS = visc_side_stride<P>();
   constexpr int TS = trace_side_stride<P, 9, R>();
-  __shared__ AvSmem<P, R> sm_all[EPB];
-  __shared__ double sT[PP], sdg[PP], sb[2 * P], sw[P];
-  __shared__ float sW1[kMlpHidden * kMlpIn], sW2[kMlpHidden * kMlpHidden], sw3[kMlpHidden], sB[kMlpFloats];
-
+  __shared__ GradSmem<P, R> sm_all[EPB];
+  __shared__ double sdg[PP], sb[2 * P], sw[P];
   const int tid = threadIdx.x;
   const int slot = tid / PP;
   const int t = tid - slot * PP;
   const int i = t % P, j = t / P;
-  AvSmem<P, R>& sm = sm_all[slot];
-  const bool mlp = (a.mode == AV_MLP) && (P >= 6);
-
-  for (int k = tid; k < PP; k += blockDim.x) {
-    sT[k] = a.T[k];
-    sdg[k] = a.dgM[k];
-  }
+  GradSmem<P, R>& sm = sm_all[slot];
+  for (int k = tid; k < PP; k += blockDim.x) sdg[k] = a.dgM[k];
   for (int k = tid; k < 2 * P; k += blockDim.x) sb[k] = a.bM[k];
   for (int k = tid; k < P; k += blockDim.x) sw[k] = a.qw[k];
-  if (mlp) {
-    for (int k = tid; k < kMlpHidden * kMlpIn; k += blockDim.x) sW1[k] = __bfloat162float(a.mlpW[k]);
-    for (int k = tid; k < kMlpHidden * kMlpHidden; k += blockDim.x)
-      sW2[k] = __bfloat162float(a.mlpW[kMlpHidden * kMlpIn + k]);
-    for (int k = tid; k < kMlpHidden; k += blockDim.x)
-      sw3[k] = __bfloat162float(a.mlpW[kMlpHidden * kMlpIn + kMlpHidden * kMlpHidden + k]);
-    for (int k = tid; k < kMlpFloats; k += blockDim.x) sB[k] = a.mlpB[k];
-  }
-
-  const long long e = (long long)blockIdx.x * EPB + slot;
-  const bool live = e < a.nEl;
+  __syncthreads();
   const R* trIn = reinterpret_cast<const R*>(a.trIn);
-  const R gam = (R)a.gamma;
-
-  if (live) {
+  const int count = *a.activeCount;
+  // every block runs the same number of rounds (block-uniform barriers)
+  for (int base = blockIdx.x * EPB; base < count; base += gridDim.x * EPB) {
+    const bool live = base + slot < count && t < PP;
+    const long long e = live ? a.activeList[base + slot] : 0;
+    if (live) {
 #pragma unroll
-    for (int v = 0; v < 4; ++v) sm.q[v][t] = (R)a.q[t + (long long)PP * (v + 4 * e)];
-    // wave speed |u| + c at this node (src/models/SELF_CompressibleIdealGas2D.f90:1090-1110)
-    const R rho = sm.q[2][t], u = sm.q[0][t] / rho, v = sm.q[1][t] / rho;
-    const R ke = (R)0.5 * (sm.q[0][t] * u + sm.q[1][t] * v);
-    const R p = (gam - (R)1) * (sm.q[3][t] - ke);
-    const R c = av_sqrt<R>(gam * p / rho);
-    sm.lam[t] = av_sqrt<R>(u * u + v * v) + c;
-  }
-  __syncthreads();
-  // modal transform, pass 1: tt(k, j) = sum_i T(k,i) q(i,j) (density, and total energy for the MLP)
-  if (live) {
-    const int k = i, jj = j;
+      for (int v = 0; v < 4; ++v) sm.q[v][t] = (R)a.q[t + (long long)PP * (v + 4 * e)];
+      const double* gd = a.dsdx + 4 * (t + (long long)PP * e);
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      if (r == 1 && !mlp) break;
-      const R* qv = sm.q[2 + r];
-      R acc = (R)0;
+      for (int k = 0; k < 4; ++k) sm.dsdx[k][t] = (R)gd[k];
+      // averaged conservative traces (BassiRebaySides) with the stage's exterior states
+      for (int k = t; k < 4 * P; k += PP) {
+        const int s1 = k / P, ii = k % P;
+        const int* si = a.sideInfo + 5 * (s1 + 4 * e);
+        const R* own = trIn + (long long)TS * (s1 + 4 * e);
+        R L[4], X[4];
 #pragma unroll
-      for (int m = 0; m < P; ++m) acc = acc + (R)sT[k + P * m] * qv[m + P * jj];
-      sm.tt[r][k + P * jj] = acc;
-    }
-  }
-  __syncthreads();
-  // pass 2: c(k, l) = sum_j T(l,j) tt(k,j)
-  if (live) {
-    const int k = i, l = j;
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      if (r == 1 && !mlp) break;
-      R acc = (R)0;
-#pragma unroll
-      for (int m = 0; m < P; ++m) acc = acc + (R)sT[l + P * m] * sm.tt[r][k + P * m];
-      sm.c[r][k + P * l] = acc;
-    }
-  }
-  __syncthreads();
-  // modal energies c^2 in place
-  if (live) {
-    sm.c[0][t] = sm.c[0][t] * sm.c[0][t];
-    if (mlp) sm.c[1][t] = sm.c[1][t] * sm.c[1][t];
-  }
-  __syncthreads();
-  // fixed-order partial sums per eta-degree l: all modes, the highest-shell
-  // modes (k = N or l = N), and the wave-speed maximum over the node column
-  if (live && t < P) {
-    const int l = t;
-    R tot = (R)0, tot1 = (R)0, lmax = (R)0;
-#pragma unroll
-    for (int k = 0; k < P; ++k) {
-      tot = tot + sm.c[0][k + P * l];
-      if (mlp) tot1 = tot1 + sm.c[1][k + P * l];
-      const R w = sm.lam[k + P * l];
-      if (w > lmax) lmax = w;
-    }
-    sm.part[0][l] = tot;
-    sm.part[1][l] = (l == N) ? tot : sm.c[0][N + P * l];
-    sm.part[2][l] = tot1;
-    sm.part[3][l] = lmax;
-  }
-  __syncthreads();
-  if (live && t < 2) {
-    R total = (R)0, top = (R)0, lam = (R)0;
-#pragma unroll
-    for (int l = 0; l < P; ++l) {
-      total = total + sm.part[t == 0 ? 0 : 2][l];
-      top = top + sm.part[1][l];
-      if (sm.part[3][l] > lam) lam = sm.part[3][l];
-    }
-    sm.tot[t] = total;
-    if (t == 0) {
-      R act = (R)0;  // modal decay activation of the density
-      int need = 0;
-      if (top > (R)0 && total > (R)0) {
-        const R sv = av_log10<R>(top / total);
-        if (sv > (R)a.s0 + (R)a.kappa) act = (R)1;
-        else if (!(sv < (R)a.s0 - (R)a.kappa))
-          act = (R)0.5 * ((R)1 + av_sin<R>((R)kAvPi * (sv - (R)a.s0) / ((R)2 * (R)a.kappa)));
-        need = !(sv < (R)(a.s0 - a.kappa - kMlpGate));
-      }
-      sm.actInd = act;
-      sm.lamMax = lam;
-      sm.needMlp = mlp && need;
-    }
-  }
-  // the MLP phase runs when any element of the block needs it (block-uniform barriers)
-  const bool anyMlp = __syncthreads_or(live && mlp && sm.needMlp) != 0;
-  if (anyMlp) {
-    const bool run = live && sm.needMlp;
-    // one thread per feature: energy fraction of one high shell max(k,l) = m, xi-degree k = m or
-    // eta-degree l = m (m = N-5..N) of the density (features 0..17) or total energy (18..35)
-    if (run && t < kMlpIn) {
-      const int r = t / 18, grp = (t % 18) / 6, m = N - 5 + t % 6;
-      const R* e2 = sm.c[r];
-      R sum = (R)0;
-      if (grp == 0) {
-        for (int l = 0; l < m; ++l) sum = sum + e2[m + P * l];
-        for (int k = 0; k <= m; ++k) sum = sum + e2[k + P * m];
-      } else if (grp == 1) {
-        for (int l = 0; l < P; ++l) sum = sum + e2[m + P * l];
-      } else {
-        for (int k = 0; k < P; ++k) sum = sum + e2[k + P * m];
-      }
-      const R total = sm.tot[r];
-      R qf = total > (R)0 ? sum / total : (R)0;
-      if (qf < (R)1e-16) qf = (R)1e-16;
-      sm.feat[t] = (float)((av_log10<R>(qf) + (R)8) / (R)8);
-    }
-    __syncthreads();
-    if (run && t < kMlpHidden) {
-      float acc = 0.f;
-#pragma unroll 4
-      for (int k = 0; k < kMlpIn; ++k) acc = fmaf(sW1[t * kMlpIn + k], sm.feat[k], acc);
-      acc = acc + sB[t];
-      sm.h1[t] = acc > 0.f ? acc : 0.f;
-    }
-    __syncthreads();
-    if (run && t < kMlpHidden) {
-      float acc = 0.f;
-#pragma unroll 4
-      for (int k = 0; k < kMlpHidden; ++k) acc = fmaf(sW2[t * kMlpHidden + k], sm.h1[k], acc);
-      acc = acc + sB[kMlpHidden + t];
-      sm.h2[t] = acc > 0.f ? acc : 0.f;
-    }
-    __syncthreads();
-  }
-  if (live && t == 0) {
-    const R actInd = sm.actInd;
-    R act = actInd;
-    if (mlp && sm.needMlp) {
-      if (a.fallbacks) atomicAdd(a.fallbacks + 1, 1);
-      bool inRange = true;
-      const float* fmin = sB + 2 * kMlpHidden + 1;
-      const float* fmax = fmin + kMlpIn;
-      for (int k = 0; k < kMlpIn; ++k)
-        inRange = inRange && sm.feat[k] >= fmin[k] - kMlpRangeMargin && sm.feat[k] <= fmax[k] + kMlpRangeMargin;
-      if (inRange) {
-        float z = 0.f;
-        for (int k = 0; k < kMlpHidden; ++k) z = fmaf(sw3[k], sm.h2[k], z);
-        z = z + sB[2 * kMlpHidden];
-        act = (R)(z < 0.f ? 0.f : (z > 1.f ? 1.f : z));
-      } else if (a.fallbacks) {
-        atomicAdd(a.fallbacks, 1);
-      }
-    }
-    if (mlp && a.actInd) a.actInd[e] = (float)actInd;
-    const double nu = (double)act * a.avC * a.hEl[e] / (double)N * (double)sm.lamMax;
-    sm.nu = (R)nu;
-    sm.active = nu != 0.0;
-    a.nu[e] = nu;
-    a.act[e] = (float)act;
-  }
-  __syncthreads();
-  // Elements with nu = 0 contribute exact zeros (zero viscous flux and zero
-  // viscous traces); they stop here and the stage kernel skips them, so the
-  // viscous work scales with the shocked region.
-  const bool active = live && sm.active;
-  if (active) {
-    const double* gd = a.dsdx + 4 * (t + (long long)PP * e);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) sm.dsdx[k][t] = (R)gd[k];
-    // averaged conservative traces (BassiRebaySides) with the stage's exterior states
-    for (int k = t; k < 4 * P; k += PP) {
-      const int s1 = k / P, ii = k % P;
-      const int* si = a.sideInfo + 5 * (s1 + 4 * e);
-      const R* own = trIn + (long long)TS * (s1 + 4 * e);
-      R L[4], X[4];
-#pragma unroll
-      for (int w = 0; w < 4; ++w) {
-        L[w] = own[ii + P * w];
-        X[w] = (R)0;
-      }
-      const int bcid = si[4];
-      if (bcid == 0) {
-        const long long e2 = si[2] - 1;
-        const int s2 = si[3] / 10 - 1, flip = si[3] % 10;
-        const R* nb = trIn + (long long)TS * (s2 + 4 * e2);
-        const int i2 = flip ? N - ii : ii;
-#pragma unroll
-        for (int w = 0; w < 4; ++w) X[w] = nb[i2 + P * w];
-      } else if (si[2] == 0) {  // physical side: the boundary condition's exterior state
-        if (bcid == SG_BC_NONORMALFLOW) {
-          const double2 nh = reinterpret_cast<const double2*>(a.nHat)[ii + (long long)P * (s1 + 4 * e)];
-          reflect<R>(L[0], L[1], nh.x, nh.y, X[0], X[1]);
-          X[2] = L[2];
-          X[3] = L[3];
-        } else if ((bcid == SG_BC_PRESCRIBED || bcid == SG_BC_RADIATION) && a.presc) {
-#pragma unroll
-          for (int w = 0; w < 4; ++w) X[w] = (R)a.presc[ii + (long long)P * (w + 4 * (s1 + 4 * e))];
+        for (int w = 0; w < 4; ++w) {
+          L[w] = own[ii + P * w];
+          X[w] = (R)0;
         }
-      }
+        const int bcid = si[4];
+        if (bcid == 0) {
+          const long long e2 = si[2] - 1;
+          const int s2 = si[3] / 10 - 1, flip = si[3] % 10;
+          const R* nb = trIn + (long long)TS * (s2 + 4 * e2);
+          const int i2 = flip ? N - ii : ii;
 #pragma unroll
-      for (int w = 0; w < 4; ++w) sm.avg[s1][w][ii] = (R)0.5 * (L[w] + X[w]);
+          for (int w = 0; w < 4; ++w) X[w] = nb[i2 + P * w];
+        } else if (si[2] == 0) {  // physical side: the boundary condition's exterior state
+          if (bcid == SG_BC_NONORMALFLOW) {
+            const double2 nh = reinterpret_cast<const double2*>(a.nHat)[ii + (long long)P * (s1 + 4 * e)];
+            reflect<R>(L[0], L[1], nh.x, nh.y, X[0], X[1]);
+            X[2] = L[2];
+            X[3] = L[3];
+          } else if ((bcid == SG_BC_PRESCRIBED || bcid == SG_BC_RADIATION) && a.presc) {
+#pragma unroll
+            for (int w = 0; w < 4; ++w) X[w] = (R)a.presc[ii + (long long)P * (w + 4 * (s1 + 4 * e))];
+          }
+        }
+#pragma unroll
+        for (int w = 0; w < 4; ++w) sm.avg[s1][w][ii] = (R)0.5 * (L[w] + X[w]);
+      }
     }
-  }
-  __syncthreads();
-  // BR1 gradient (GradientBR_MappedScalar2D, src/SELF_MappedData.f90:990-1074) scaled by nu,
-  // and the contravariant viscous flux (src/models/hip/SELF_Advection2D.cpp:66-95)
-  if (active) {
-    const R nu = sm.nu;
-    const double* nH = a.nHat + 2 * (long long)P * 4 * e;
-    const double* nS = a.nScale + (long long)P * 4 * e;
-    const R Jij = (R)a.J[t + (long long)PP * e];
-    R* visc = reinterpret_cast<R*>(a.visc);
+    __syncthreads();
+    // BR1 gradient (GradientBR_MappedScalar2D, src/SELF_MappedData.f90:990-1074) scaled by nu,
+    // and the contravariant viscous flux (src/models/hip/SELF_Advection2D.cpp:66-95)
+    if (live) {
+      const R nu = (R)a.nu[e];
+      const double* nH = a.nHat + 2 * (long long)P * 4 * e;
+      const double* nS = a.nScale + (long long)P * 4 * e;
+      const R Jij = (R)a.J[t + (long long)PP * e];
+      R* visc = reinterpret_cast<R*>(a.visc);
 #pragma unroll 1
-    for (int v = 0; v < 4; ++v) {
-      R gx = (R)0, gy = (R)0;
+      for (int v = 0; v < 4; ++v) {
+        R gx = (R)0, gy = (R)0;
 #pragma unroll
-      for (int ii = 0; ii < P; ++ii) {
-        const R qa = sm.q[v][ii + P * j], qb = sm.q[v][i + P * ii];
-        R f1 = qa * sm.dsdx[0][ii + P * j];
-        R f2 = qb * sm.dsdx[2][i + P * ii];
-        gx = gx + (R)sdg[ii + P * i] * f1 + (R)sdg[ii + P * j] * f2;
-        f1 = qa * sm.dsdx[1][ii + P * j];
-        f2 = qb * sm.dsdx[3][i + P * ii];
-        gy = gy + (R)sdg[ii + P * i] * f1 + (R)sdg[ii + P * j] * f2;
+        for (int ii = 0; ii < P; ++ii) {
+          const R qa = sm.q[v][ii + P * j], qb = sm.q[v][i + P * ii];
+          R f1 = qa * sm.dsdx[0][ii + P * j];
+          R f2 = qb * sm.dsdx[2][i + P * ii];
+          gx = gx + (R)sdg[ii + P * i] * f1 + (R)sdg[ii + P * j] * f2;
+          f1 = qa * sm.dsdx[1][ii + P * j];
+          f2 = qb * sm.dsdx[3][i + P * ii];
+          gy = gy + (R)sdg[ii + P * i] * f1 + (R)sdg[ii + P * j] * f2;
+        }
+        // nHat(d, k, side) at nH[d + 2 (k + P side)], nScale(k, side) at nS[k + P side]
+        R f1 = sm.avg[1][v][j] * (R)nH[0 + 2 * (j + P * 1)] * (R)nS[j + P * 1];
+        R f2 = sm.avg[3][v][j] * (R)nH[0 + 2 * (j + P * 3)] * (R)nS[j + P * 3];
+        gx = gx + (f1 * (R)sb[i + P] + f2 * (R)sb[i]) / (R)sw[i];
+        f1 = sm.avg[2][v][i] * (R)nH[0 + 2 * (i + P * 2)] * (R)nS[i + P * 2];
+        f2 = sm.avg[0][v][i] * (R)nH[0 + 2 * (i + P * 0)] * (R)nS[i + P * 0];
+        gx = gx + (f1 * (R)sb[j + P] + f2 * (R)sb[j]) / (R)sw[j];
+        f1 = sm.avg[1][v][j] * (R)nH[1 + 2 * (j + P * 1)] * (R)nS[j + P * 1];
+        f2 = sm.avg[3][v][j] * (R)nH[1 + 2 * (j + P * 3)] * (R)nS[j + P * 3];
+        gy = gy + (f1 * (R)sb[i + P] + f2 * (R)sb[i]) / (R)sw[i];
+        f1 = sm.avg[2][v][i] * (R)nH[1 + 2 * (i + P * 2)] * (R)nS[i + P * 2];
+        f2 = sm.avg[0][v][i] * (R)nH[1 + 2 * (i + P * 0)] * (R)nS[i + P * 0];
+        gy = gy + (f1 * (R)sb[j + P] + f2 * (R)sb[j]) / (R)sw[j];
+        gx = gx / Jij;
+        gy = gy / Jij;
+        gx = gx * nu;
+        gy = gy * nu;
+        sm.g[0][v][t] = gx;
+        sm.g[1][v][t] = gy;
+        const R c1 = -(sm.dsdx[0][t] * gx + sm.dsdx[1][t] * gy);
+        const R c2 = -(sm.dsdx[2][t] * gx + sm.dsdx[3][t] * gy);
+        visc[t + (long long)PP * (0 + 2 * (v + 4 * e))] = c1;
+        visc[t + (long long)PP * (1 + 2 * (v + 4 * e))] = c2;
       }
-      // nHat(d, k, side) at nH[d + 2 (k + P side)], nScale(k, side) at nS[k + P side]
-      R f1 = sm.avg[1][v][j] * (R)nH[0 + 2 * (j + P * 1)] * (R)nS[j + P * 1];
-      R f2 = sm.avg[3][v][j] * (R)nH[0 + 2 * (j + P * 3)] * (R)nS[j + P * 3];
-      gx = gx + (f1 * (R)sb[i + P] + f2 * (R)sb[i]) / (R)sw[i];
-      f1 = sm.avg[2][v][i] * (R)nH[0 + 2 * (i + P * 2)] * (R)nS[i + P * 2];
-      f2 = sm.avg[0][v][i] * (R)nH[0 + 2 * (i + P * 0)] * (R)nS[i + P * 0];
-      gx = gx + (f1 * (R)sb[j + P] + f2 * (R)sb[j]) / (R)sw[j];
-      f1 = sm.avg[1][v][j] * (R)nH[1 + 2 * (j + P * 1)] * (R)nS[j + P * 1];
-      f2 = sm.avg[3][v][j] * (R)nH[1 + 2 * (j + P * 3)] * (R)nS[j + P * 3];
-      gy = gy + (f1 * (R)sb[i + P] + f2 * (R)sb[i]) / (R)sw[i];
-      f1 = sm.avg[2][v][i] * (R)nH[1 + 2 * (i + P * 2)] * (R)nS[i + P * 2];
-      f2 = sm.avg[0][v][i] * (R)nH[1 + 2 * (i + P * 0)] * (R)nS[i + P * 0];
-      gy = gy + (f1 * (R)sb[j + P] + f2 * (R)sb[j]) / (R)sw[j];
-      gx = gx / Jij;
-      gy = gy / Jij;
-      gx = gx * nu;
-      gy = gy * nu;
-      sm.g[0][v][t] = gx;
-      sm.g[1][v][t] = gy;
-      const R c1 = -(sm.dsdx[0][t] * gx + sm.dsdx[1][t] * gy);
-      const R c2 = -(sm.dsdx[2][t] * gx + sm.dsdx[3][t] * gy);
-      visc[t + (long long)PP * (0 + 2 * (v + 4 * e))] = c1;
-      visc[t + (long long)PP * (1 + 2 * (v + 4 * e))] = c2;
     }
-  }
-  __syncthreads();
-  // face traces of nu grad q (VectorBoundaryInterp_2D, src/SELF_Lagrange.f90:2284-2316)
-  if (active) {
-    R* vo = reinterpret_cast<R*>(a.vtr) + (long long)4 * VS * e;
-    for (int k = t; k < 4 * 8 * P; k += PP) {
-      const int ii = k % P, d = (k / P) % 2, v = (k / (2 * P)) % 4, s1 = k / (8 * P);
-      vo[s1 * VS + ii + P * (d + 2 * v)] = face_trace<P, R>(sm.g[d][v], sb, s1, ii);
+    __syncthreads();
+    // face traces of nu grad q (VectorBoundaryInterp_2D, src/SELF_Lagrange.f90:2284-2316)
+    if (live) {
+      R* vo = reinterpret_cast<R*>(a.vtr) + (long long)4 * VS * e;
+      for (int k = t; k < 4 * 8 * P; k += PP) {
+        const int ii = k % P, d = (k / P) % 2, v = (k / (2 * P)) % 4, s1 = k / (8 * P);
+        vo[s1 * VS + ii + P * (d + 2 * v)] = face_trace<P, R>(sm.g[d][v], sb, s1, ii);
+      }
     }
+    __syncthreads();  // the slot's arrays are reused by the next round
   }
 }
 
@@ -499,25 +525,29 @@ struct QwArr {
   double w[kMaxP];
 };
 
+template <int P, typename R>
+cudaError_t launch_av_pair(const AvArgs& a, cudaStream_t st, int numSMs) {
+  cudaError_t e = cudaMemsetAsync(a.activeCount, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  const long long nuBlocks = (a.nEl + kNuWarps - 1) / kNuWarps;
+  const int g1 = (int)(nuBlocks < 16LL * numSMs ? nuBlocks : 16LL * numSMs);
+  k_av_nu<P, R><<<g1, 32 * kNuWarps, 0, st>>>(a);
+  constexpr int EPB = av_elems_per_block<P, R>();
+  k_av_grad<P, R, EPB><<<4 * numSMs, EPB * P * P, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
 template <typename R>
-cudaError_t launch_av_prep_impl(int P, const AvArgs& a, cudaStream_t st) {
+cudaError_t launch_av_prep_impl(int P, const AvArgs& a, cudaStream_t st, int numSMs) {
   switch (P) {
-#define SG_AV_CASE(PV)                                                                         \
-  case PV: {                                                                                   \
-    constexpr int EPB = av_elems_per_block<PV, R>();                                           \
-    k_av_prep<PV, R, EPB><<<(a.nEl + EPB - 1) / EPB, EPB * PV * PV, 0, st>>>(a);                \
-    return cudaGetLastError();                                                                 \
-  }
-    SG_AV_CASE(2)
-    SG_AV_CASE(3)
-    SG_AV_CASE(4)
-    SG_AV_CASE(5)
-    SG_AV_CASE(6)
-    SG_AV_CASE(7)
-    SG_AV_CASE(8)
-#undef SG_AV_CASE
-    default:
-      return cudaErrorInvalidValue;
+    case 2: return launch_av_pair<2, R>(a, st, numSMs);
+    case 3: return launch_av_pair<3, R>(a, st, numSMs);
+    case 4: return launch_av_pair<4, R>(a, st, numSMs);
+    case 5: return launch_av_pair<5, R>(a, st, numSMs);
+    case 6: return launch_av_pair<6, R>(a, st, numSMs);
+    case 7: return launch_av_pair<7, R>(a, st, numSMs);
+    case 8: return launch_av_pair<8, R>(a, st, numSMs);
+    default: return cudaErrorInvalidValue;
   }
 }
 

@@ -105,7 +105,7 @@ struct selfgpu_model2d {
   AvArgs av{};
   double* avNu = nullptr;
   float* avAct = nullptr;  // [0, nEl): activation applied, [nEl, 2 nEl): indicator activation
-  int* avFallbacks = nullptr;
+  int* avFallbacks = nullptr;  // [0] MLP fallbacks, [1] MLP evaluations, [2] active count, then the active list
   double* avH = nullptr;
   void* avVisc = nullptr;
   void* avVtr = nullptr;
@@ -129,8 +129,9 @@ struct selfgpu_model2d {
     x.trIn = trIn;
     x.presc = base.fld[2];
     x.gamma = base.gamma;
-    ++launches;
-    return form == SELFGPU_FP64 ? launch_av_prep_fp64(P, x, stream) : launch_av_prep_fp32(P, x, stream);
+    launches += 2;
+    return form == SELFGPU_FP64 ? launch_av_prep_fp64(P, x, stream, cfg.numSMs)
+                                : launch_av_prep_fp32(P, x, stream, cfg.numSMs);
   }
 
   cudaError_t launch(StageArgs a) {
@@ -663,7 +664,7 @@ int selfgpu_model2d_set_closure(selfgpu_model2d* m, int mode, double c, double s
   if (!m->avNu) {
     e = cudaMalloc(&m->avNu, nEl * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&m->avAct, 2 * nEl * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&m->avFallbacks, 2 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&m->avFallbacks, (3 + nEl) * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&m->avH, nEl * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&m->avVisc, 8 * PP * nEl * m->elemBytes());
     if (e == cudaSuccess) e = cudaMalloc(&m->avVtr, 4 * 8 * (size_t)m->P * nEl * m->elemBytes());
@@ -685,6 +686,8 @@ int selfgpu_model2d_set_closure(selfgpu_model2d* m, int mode, double c, double s
   x.act = m->avAct;
   x.actInd = m->avAct + nEl;
   x.fallbacks = m->avFallbacks;
+  x.activeCount = m->avFallbacks + 2;
+  x.activeList = m->avFallbacks + 3;
   x.visc = m->avVisc;
   x.vtr = m->avVtr;
   x.mlpW = m->mlpW;

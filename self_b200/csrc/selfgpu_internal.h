@@ -44,8 +44,9 @@ cudaError_t launch_stage_fp32(int model, int P, const StageArgs& a, const StageL
                               int* usedTma);
 // Artificial-viscosity closure (av_closure.cuh).
 struct AvArgs;
-cudaError_t launch_av_prep_fp64(int P, const AvArgs& a, cudaStream_t st);
-cudaError_t launch_av_prep_fp32(int P, const AvArgs& a, cudaStream_t st);
+// closure: the viscosity kernel and the viscous-term kernel of one stage
+cudaError_t launch_av_prep_fp64(int P, const AvArgs& a, cudaStream_t st, int numSMs);
+cudaError_t launch_av_prep_fp32(int P, const AvArgs& a, cudaStream_t st, int numSMs);
 cudaError_t launch_element_size(const double* J, const double* qw, int P, int nEl, double* h, cudaStream_t st);
 cudaError_t launch_closure_features(const double* q, int P, int nEl, const AvArgs& a, float* act, float* feat,
                                     cudaStream_t st);

@@ -9,5 +9,7 @@ cudaError_t launch_stage_fp32(int model, int P, const StageArgs& a, const StageL
                               int* usedTma) {
   return launch_stage_impl<float>(model, P, a, L, st, usedTma);
 }
-cudaError_t launch_av_prep_fp32(int P, const AvArgs& a, cudaStream_t st) { return launch_av_prep_impl<float>(P, a, st); }
+cudaError_t launch_av_prep_fp32(int P, const AvArgs& a, cudaStream_t st, int numSMs) {
+  return launch_av_prep_impl<float>(P, a, st, numSMs);
+}
 }  // namespace selfgpu

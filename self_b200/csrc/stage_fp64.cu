@@ -11,7 +11,9 @@ cudaError_t launch_stage_fp64(int model, int P, const StageArgs& a, const StageL
   return launch_stage_impl<double>(model, P, a, L, st, usedTma);
 }
 
-cudaError_t launch_av_prep_fp64(int P, const AvArgs& a, cudaStream_t st) { return launch_av_prep_impl<double>(P, a, st); }
+cudaError_t launch_av_prep_fp64(int P, const AvArgs& a, cudaStream_t st, int numSMs) {
+  return launch_av_prep_impl<double>(P, a, st, numSMs);
+}
 
 // h = sqrt(sum_j sum_i w_i w_j J_ij), in the oracle's summation order
 __global__ void k_element_size(const double* __restrict__ J, QwArr qw, int P, int nEl, double* __restrict__ h) {
