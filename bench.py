@@ -25,6 +25,7 @@ workload, metric and unit.  Multi-GPU: the path runs as independent replicas
 the slowest rank's time.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -254,6 +255,10 @@ def _closure_variant(mesh, geo, q0, form, mode, mlp, steps, dt, dof):
         model.SetClosure(mode, c=1.0, mlp=mlp)
     model.ForwardStep(2, dt)  # captures the RK-step graph
     model.Sync()
+    p_, g_, us_ = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+    S.check(S.lib().selfgpu_model2d_autotune(model._h, ctypes.byref(p_), ctypes.byref(g_), ctypes.byref(us_)))
+    model.ForwardStep(1, dt)  # recapture with the tuned launch
+    model.Sync()
     model.SetSolution(q0)
     model.workSol.zero_()
     l0 = model.LaunchCount()
@@ -261,7 +266,8 @@ def _closure_variant(mesh, geo, q0, form, mode, mlp, steps, dt, dof):
         model.ClosureState(reset=True)
     ms = _events_ms(lambda: model.ForwardStep(steps, dt))
     res = {"value": dof * steps / (ms / 1e3), "unit": "DOF-updates/s", "ms_per_rk3_step": ms / steps,
-           "launches_per_rk3_step": (model.LaunchCount() - l0) / steps}
+           "launches_per_rk3_step": (model.LaunchCount() - l0) / steps,
+           "kernel": ("persistent, %d groups" % g_.value) if p_.value else "per-element"}
     if mode:
         nu, act, ind, (fb, evals) = model.ClosureState(reset=True)
         res["active_elements_last_stage"] = int((act > 0).sum())
