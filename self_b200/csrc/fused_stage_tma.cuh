@@ -350,16 +350,29 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       double Src[NV];
       Phys::template source<double>(qv, na, a, Src);
       const R wi = (R)sqw[i], wj = (R)sqw[j];
+      // dgMatrix columns of this node's i and j, shared by the four variables
+      R dgi[P], dgj[P];
+#pragma unroll
+      for (int m = 0; m < P; ++m) {
+        dgi[m] = (R)sdg[m + P * i];
+        dgj[m] = (R)sdg[m + P * j];
+      }
+      // the four variables' sums advance together (independent dependency chains);
+      // each keeps the reference's order over m
+      R d[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) d[v] = (R)0;
+#pragma unroll
+      for (int m = 0; m < P; ++m) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+          d[v] = d[v] + dgi[m] * gU[v * PP + m + P * j] + dgj[m] * gU[(NV + v) * PP + i + P * m];
+      }
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        const R* F1 = gU + v * PP;
-        const R* F2 = gU + (NV + v) * PP;
-        R d = (R)0;
-#pragma unroll
-        for (int m = 0; m < P; ++m) d = d + (R)sdg[m + P * i] * F1[m + P * j] + (R)sdg[m + P * j] * F2[i + P * m];
-        d = d + ((R)sb[i + P] * gfb[(1 * NV + v) * P + j] + (R)sb[i] * gfb[(3 * NV + v) * P + j]) / wi +
-            ((R)sb[j + P] * gfb[(2 * NV + v) * P + i] + (R)sb[j] * gfb[(0 * NV + v) * P + i]) / wj;
-        dsdt[v] = Src[v] - (double)d / Jij;
+        const R dv = d[v] + ((R)sb[i + P] * gfb[(1 * NV + v) * P + j] + (R)sb[i] * gfb[(3 * NV + v) * P + j]) / wi +
+                     ((R)sb[j + P] * gfb[(2 * NV + v) * P + i] + (R)sb[j] * gfb[(0 * NV + v) * P + i]) / wj;
+        dsdt[v] = Src[v] - (double)dv / Jij;
       }
     }
     if (!rk) {
