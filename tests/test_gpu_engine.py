@@ -179,16 +179,17 @@ def test_c2_full_size_tendency_and_steps():
 
 
 @pytest.mark.parametrize("model", ["LSW", "SW", "CIG"])
-def test_persistent_kernel_matches_per_element_kernel_bitwise(model):
+@pytest.mark.parametrize("N", [3, 7])
+def test_persistent_kernel_matches_per_element_kernel_bitwise(model, N):
     """The persistent bulk-copy kernel and the per-element-group kernel compute
     the same values: bit-identical states after RK3 steps."""
     import self_b200 as S
-    N, n, dt = 7, 6, 1e-3
+    n, dt = 6, 1e-3
     mesh_kind = "periodic" if model == "CIG" else "flipped"
     outs = []
     for persistent in (1, 0):
         _, mod, _, _ = build_pair(model, mesh_kind, N, seed=5)
-        S.lib().selfgpu_model2d_set_kernel(mod._h, persistent)
+        S.check(S.lib().selfgpu_model2d_set_launch(mod._h, persistent, 0))
         mod.ForwardStep(n, dt)
         mod.Sync()
         if persistent:
