@@ -164,6 +164,101 @@ def cpu_baseline(seconds=12.0, max_steps=STEPS_PER_SOLVE):
                       f"{el:.1f} s, C++ restatement of the reference CPU branches, OpenMP over elements"}
 
 
+def _cpu_rate(make_model, dof, dt, steps, threads, reps=3):
+    """Median over reps of DOF-updates/s of `steps` RK3 steps of the oracle."""
+    from oracle import oracle as O
+    O.set_threads(threads, fast=True)
+    mod = make_model()
+    mod.rk3(1, dt)  # warm-up
+    rates = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        mod.rk3(steps, dt)
+        rates.append(dof * steps / (time.perf_counter() - t0))
+    return statistics.median(rates)
+
+
+def run_cpu_table():
+    """CPU baseline table for configs C1-C5 (the oracle port, FP64 plain, no
+    closure): single thread and all host cores, median of 3 bounded samples."""
+    from oracle import build as obuild
+    obuild.build()
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+
+    def cig(nx, Nd, amp, ic):
+        def make():
+            m = O.Mesh(nx, nx, periodic=(True, True), amp=amp)
+            mod = O.Model(O.CIG, Nd, m, fast=True)
+            x = O.Geometry(Nd, m).x
+            mod.set("solution", ic(x))
+            return mod
+        return make
+
+    def smooth(x):
+        X, Y = x[0, :, :, 0, :], x[1, :, :, 0, :]
+        q = np.zeros(X.shape[:2] + (4, X.shape[2]), order="F")
+        rho = 1 + 0.1 * np.sin(2 * np.pi * X) * np.sin(2 * np.pi * Y)
+        q[:, :, 0], q[:, :, 1], q[:, :, 2] = rho * 0.5, rho * 0.3, rho
+        q[:, :, 3] = 1 / (GAMMA - 1) + 0.5 * rho * 0.34
+        return q
+
+    def lsw():
+        m = O.Mesh(10, 10, bcid=O.BC_NONORMALFLOW)
+        mod = O.Model(O.LSW, 7, m, fast=True)
+        x = O.Geometry(7, m).x
+        X, Y = x[0, :, :, 0, :], x[1, :, :, 0, :]
+        P7 = 8
+        mod.set("H", np.ones((P7, P7, 1, 100), order="F"))
+        mod.set("fCori", np.zeros((P7, P7, 1, 100), order="F"))
+        q = np.zeros((P7, P7, 3, 100), order="F")
+        q[:, :, 2] = 0.01 * np.exp(-((X - 0.5) ** 2 + (Y - 0.5) ** 2) / 0.01)
+        mod.set("solution", q)
+        return mod
+
+    rows = {}
+    specs = [
+        ("C1", "LSW 10x10 N=7 walls (gravity-wave release), dt=1e-4", lsw, 3 * 64 * 100, 1e-4, (200, 1000), None),
+        ("C2", "CIG periodic 128x128 perturbed N=7, density wave", cig(128, 7, 0.02, smooth), 4 * 64 * 16384, 1e-5,
+         (1, 5), None),
+        ("C4", "CIG periodic 256x256 N=5 (sampled on 128x128: the rate per DOF-update does not depend on the mesh "
+               "size)", cig(128, 5, 0.0, smooth), 4 * 36 * 16384, 1e-5, (1, 8), None),
+        ("C5", "CIG periodic 512x512 perturbed N=7 (sampled on 128x128, as C2)", cig(128, 7, 0.02, smooth),
+         4 * 64 * 16384, 1e-5, (1, 5), None),
+    ]
+    for name, desc, make, dof, dt, (s1, sN), _ in specs:
+        rows[name] = {"workload": desc, "one_thread": _cpu_rate(make, dof, dt, s1, 1),
+                      "all_cores": _cpu_rate(make, dof, dt, sN, cores), "cores": cores}
+    # C3: the ensemble instances, advanced one by one (a sample of the 256)
+    from self_b200 import ensemble as E
+    inst = E.make_instances(256, seed=0)[:12]
+
+    def ens_rate(threads):
+        O.set_threads(threads, fast=True)
+        tot_dof, tot_t = 0, 0.0
+        for it in inst:
+            om = O.Mesh(it.nx, it.ny, bcid=O.BC_NONORMALFLOW)
+            mod = O.Model(O.SW, it.N, om, fast=True)
+            x = O.Geometry(it.N, om).x
+            X, Y = x[0, :, :, 0, :], x[1, :, :, 0, :]
+            Pn = it.N + 1
+            mod.set("topography", E.topography(it, X, Y).reshape(Pn, Pn, 1, -1, order="F"))
+            q = np.zeros((Pn, Pn, 3, it.nElem), order="F")
+            q[:, :, 2] = E.thickness(it, X, Y)
+            mod.set("solution", q)
+            mod.rk3(1, 1e-4)
+            t0 = time.perf_counter()
+            mod.rk3(3, 1e-4)
+            tot_t += time.perf_counter() - t0
+            tot_dof += it.dof() * 3
+        return tot_dof / tot_t
+
+    rows["C3"] = {"workload": "256 SW instances (sample: the first 12, advanced one by one)",
+                  "one_thread": statistics.median([ens_rate(1) for _ in range(3)]),
+                  "all_cores": statistics.median([ens_rate(cores) for _ in range(3)]), "cores": cores}
+    return rows
+
+
 def run_forms(steps=20, err_steps=500, n_instances=256):
     """The ensemble workload: 256 seeded nonlinear ShallowWater instances
     (nx, ny ~ U{8..64}, N ~ U{3,5,7}, 4-Gaussian topography, reflecting walls,
@@ -246,8 +341,11 @@ def shock_band(x, rng):
     return q
 
 
-def _closure_variant(mesh, geo, q0, form, mode, mlp, steps, dt, dof):
-    """One timed run from q0: DOF-updates/s, the final state and closure statistics."""
+def _closure_variant(mesh, geo, q0, form, mode, mlp, steps, dt, dof, nvtx=None):
+    """One timed run from q0: DOF-updates/s, the final state and closure statistics
+    (the timed steps inside an NVTX range named nvtx, for profilers)."""
+    import torch
+
     import self_b200 as S
     model = S.CompressibleIdealGas2D(mesh, geo, form=form)
     model.SetSolution(q0)
@@ -264,7 +362,11 @@ def _closure_variant(mesh, geo, q0, form, mode, mlp, steps, dt, dof):
     l0 = model.LaunchCount()
     if mode:
         model.ClosureState(reset=True)
+    if nvtx:
+        torch.cuda.nvtx.range_push(nvtx)
     ms = _events_ms(lambda: model.ForwardStep(steps, dt))
+    if nvtx:
+        torch.cuda.nvtx.range_pop()
     res = {"value": dof * steps / (ms / 1e3), "unit": "DOF-updates/s", "ms_per_rk3_step": ms / steps,
            "launches_per_rk3_step": (model.LaunchCount() - l0) / steps,
            "kernel": ("persistent, %d groups" % g_.value) if p_.value else "per-element"}
@@ -280,15 +382,11 @@ def _closure_variant(mesh, geo, q0, form, mode, mlp, steps, dt, dof):
     return res, sol
 
 
-def run_closure_forms(n_problems=16, snapshots=4, c4_steps=50, c5_steps=100):
-    """The learned shock closure (form 4) and the large single solve with all
-    forms: training data from FP64 N=7 runs, training, the C4 workload
-    (CIG 256x256 N=5 FP32, seeded four-quadrant Riemann problem) and the C5
-    workload (CIG 512x512 N=7, smooth density wave + shock-tube band), plus
-    the C2 solve in the FP32-bulk form."""
+def train_closures(n_problems=16, snapshots=4):
+    """Training data from FP64 N=7 indicator-closure runs and the two closure
+    MLPs (N=5 from states interpolated to N=5, N=7)."""
     import torch
 
-    import self_b200 as S
     from self_b200 import closure as CL
     out = {}
     t0 = time.perf_counter()
@@ -310,65 +408,58 @@ def run_closure_forms(n_problems=16, snapshots=4, c4_steps=50, c5_steps=100):
         out[f"training_N{d}"] = {"samples": int(f.shape[0]), "active_fraction": float((l > 0).float().mean()),
                                  "epochs": 8, "batch": 8192, "mse_first_last": [float(loss[0]), float(loss[-1])],
                                  "mean_abs_err_vs_indicator": float((pred - l).abs().mean()), "seconds": tt}
-    del data
+    return out, mlps
 
-    # C4: 256 x 256, N = 5, FP32 bulk, seeded Riemann problem, learned closure
-    N4 = 5
-    interp = S.Lagrange(N4, S.GAUSS, N4, S.UNIFORM)
+
+def _closure_workload(tag, mesh, geo, q0, dt, dof, steps, mlp, desc):
+    import self_b200 as S
+    res = {"workload": desc, "dof": dof}
+    ref = None
+    for name, form, mode, m in (("fp64_indicator", S.FP64, S.CLOSURE_INDICATOR, None),
+                                ("fp32_learned", S.FP32_BULK, S.CLOSURE_MLP, mlp),
+                                ("fp32_indicator", S.FP32_BULK, S.CLOSURE_INDICATOR, None),
+                                ("fp64_no_closure", S.FP64, S.CLOSURE_OFF, None)):
+        r, sol = _closure_variant(mesh, geo, q0, form, mode, m, steps, dt, dof, nvtx=f"{tag}_{name}")
+        if ref is None:
+            ref = sol
+        else:
+            r["rel_l2_vs_fp64_indicator"] = _rel_l2(sol, ref)
+        res[name] = r
+    res["speedup_fp32_learned_vs_fp64_no_closure"] = res["fp32_learned"]["value"] / res["fp64_no_closure"]["value"]
+    return res
+
+
+def measure_c4(mlp5, steps=50):
+    """C4: CIG periodic 256x256 N=5, seeded four-quadrant Riemann problem."""
+    import self_b200 as S
+    from self_b200 import closure as CL
+    interp = S.Lagrange(5, S.GAUSS, 5, S.UNIFORM)
     mesh = S.Mesh2D(256, 256, periodic=(True, True))
     geo = S.SEMQuad(interp, mesh)
-    rng = np.random.Generator(np.random.PCG64(100))
-    q0 = CL.riemann_quadrants(geo.x, rng)
-    dof4 = 4 * (N4 + 1) ** 2 * mesh.nElem
-    probe = S.CompressibleIdealGas2D(mesh, geo)
-    dt4 = CL.stable_dt(probe, q0)
-    del probe
-    c4 = {"workload": f"CIG periodic 256x256 N=5, seeded four-quadrant Riemann problem, {c4_steps} RK3 steps, "
-                      f"dt={dt4:.3e}", "dof": dof4}
-    ref4 = None
-    for name, form, mode, mlp in (("fp64_indicator", S.FP64, S.CLOSURE_INDICATOR, None),
-                                  ("fp32_learned", S.FP32_BULK, S.CLOSURE_MLP, mlps[5]),
-                                  ("fp32_indicator", S.FP32_BULK, S.CLOSURE_INDICATOR, None),
-                                  ("fp64_no_closure", S.FP64, S.CLOSURE_OFF, None)):
-        res, sol = _closure_variant(mesh, geo, q0, form, mode, mlp, c4_steps, dt4, dof4)
-        if ref4 is None:
-            ref4 = sol
-        else:
-            res["rel_l2_vs_fp64_indicator"] = _rel_l2(sol, ref4)
-        c4[name] = res
-    c4["speedup_fp32_learned_vs_fp64_no_closure"] = c4["fp32_learned"]["value"] / c4["fp64_no_closure"]["value"]
-    out["c4_learned_closure"] = c4
-    del ref4, q0, geo, mesh
+    q0 = CL.riemann_quadrants(geo.x, np.random.Generator(np.random.PCG64(100)))
+    dt = CL.stable_dt(S.CompressibleIdealGas2D(mesh, geo), q0)
+    return _closure_workload("c4", mesh, geo, q0, dt, 4 * 36 * mesh.nElem, steps, mlp5,
+                             f"CIG periodic 256x256 N=5, seeded four-quadrant Riemann problem, {steps} RK3 steps, "
+                             f"dt={dt:.3e}")
 
-    # C5: 512 x 512, N = 7, all forms
-    N5 = 7
-    interp = S.Lagrange(N5, S.GAUSS, N5, S.UNIFORM)
+
+def measure_c5(mlp7, steps=100):
+    """C5: CIG periodic 512x512 perturbed N=7, smooth density wave + shock-tube band."""
+    import self_b200 as S
+    from self_b200 import closure as CL
+    interp = S.Lagrange(7, S.GAUSS, 7, S.UNIFORM)
     mesh = S.Mesh2D(512, 512, periodic=(True, True), perturbation=0.02)
     geo = S.SEMQuad(interp, mesh)
-    rng = np.random.Generator(np.random.PCG64(200))
-    q0 = shock_band(geo.x, rng)
-    dof5 = 4 * (N5 + 1) ** 2 * mesh.nElem
-    probe = S.CompressibleIdealGas2D(mesh, geo)
-    dt5 = CL.stable_dt(probe, q0)
-    del probe
-    c5 = {"workload": f"CIG periodic 512x512 perturbed N=7, smooth density wave + shock-tube band, {c5_steps} RK3 "
-                      f"steps, dt={dt5:.3e}", "dof": dof5}
-    ref5 = None
-    for name, form, mode, mlp in (("fp64_indicator", S.FP64, S.CLOSURE_INDICATOR, None),
-                                  ("fp32_learned", S.FP32_BULK, S.CLOSURE_MLP, mlps[7]),
-                                  ("fp32_indicator", S.FP32_BULK, S.CLOSURE_INDICATOR, None),
-                                  ("fp64_no_closure", S.FP64, S.CLOSURE_OFF, None)):
-        res, sol = _closure_variant(mesh, geo, q0, form, mode, mlp, c5_steps, dt5, dof5)
-        if ref5 is None:
-            ref5 = sol
-        else:
-            res["rel_l2_vs_fp64_indicator"] = _rel_l2(sol, ref5)
-        c5[name] = res
-    c5["speedup_fp32_learned_vs_fp64_no_closure"] = c5["fp32_learned"]["value"] / c5["fp64_no_closure"]["value"]
-    out["c5_large_solve"] = c5
-    del ref5, q0, geo, mesh
+    q0 = shock_band(geo.x, np.random.Generator(np.random.PCG64(200)))
+    dt = CL.stable_dt(S.CompressibleIdealGas2D(mesh, geo), q0)
+    return _closure_workload("c5", mesh, geo, q0, dt, 4 * 64 * mesh.nElem, steps, mlp7,
+                             f"CIG periodic 512x512 perturbed N=7, smooth density wave + shock-tube band, {steps} RK3 "
+                             f"steps, dt={dt:.3e}")
 
-    # C2 in the FP32-bulk form (smooth: the closure stays off), error vs the FP64 engine
+
+def measure_c2_forms():
+    """C2 in the FP64 and FP32-bulk forms (smooth: no closure), FP32 error vs FP64."""
+    import self_b200 as S
     interp = S.Lagrange(N, S.GAUSS, N, S.UNIFORM)
     mesh = S.Mesh2D(NX, NX, periodic=(True, True), perturbation=0.02)
     geo = S.SEMQuad(interp, mesh)
@@ -378,14 +469,61 @@ def run_closure_forms(n_problems=16, snapshots=4, c4_steps=50, c5_steps=100):
     c2 = {}
     ref2 = None
     for name, form in (("fp64", S.FP64), ("fp32_bulk", S.FP32_BULK)):
-        res, sol = _closure_variant(mesh, geo, q0, form, S.CLOSURE_OFF, None, STEPS_PER_SOLVE, dt, DOF)
+        res, sol = _closure_variant(mesh, geo, q0, form, S.CLOSURE_OFF, None, STEPS_PER_SOLVE, dt, DOF,
+                                    nvtx=f"c2_{name}")
         if ref2 is None:
             ref2 = sol
         else:
             res["rel_l2_vs_fp64"] = _rel_l2(sol, ref2)
         c2[name] = res
     c2["speedup_fp32_bulk_vs_fp64"] = c2["fp32_bulk"]["value"] / c2["fp64"]["value"]
-    out["c2_forms"] = c2
+    return c2
+
+
+def measure_c1():
+    """C1: LinearShallowWater gravity-wave release, 10x10 walls, N=7, 1000 steps of dt = 1e-4."""
+    import torch
+
+    import self_b200 as S
+    interp = S.Lagrange(7, S.GAUSS, 7, S.UNIFORM)
+    mesh = S.Mesh2D(10, 10, bcid=S.BC_NONORMALFLOW)
+    geo = S.SEMQuad(interp, mesh)
+    lsw = S.LinearShallowWater(mesh, geo)
+    X, Y = geo.x[:, 0, :, :, 0], geo.x[:, 0, :, :, 1]
+    q1 = torch.zeros((mesh.nElem, 3, 8, 8), device="cuda", dtype=torch.float64)
+    q1[:, 2] = 0.01 * torch.exp(-((X - 0.5) ** 2 + (Y - 0.5) ** 2) / 0.01)
+    lsw.SetSolution(q1)
+    lsw.ForwardStep(10, 1e-4)
+    lsw.Sync()
+    lsw.SetSolution(q1)
+    lsw.workSol.zero_()
+    ms = _events_ms(lambda: lsw.ForwardStep(1000, 1e-4))
+    lsw.CheckFinite()
+    return {"workload": "LinearShallowWater 10x10 walls N=7, gravity-wave release, 1000 RK3 steps, dt=1e-4, FP64 "
+                        "(19,200 DOF: launch-latency bound; graph-replayed steps)",
+            "value": 19200 * 1000 / (ms / 1e3), "unit": "DOF-updates/s", "ms_per_rk3_step": ms / 1000}
+
+
+def run_closure_forms():
+    """The learned shock closure (form 4), the large single solve with all
+    forms, C2 in the FP32-bulk form and C1."""
+    out, mlps = train_closures()
+    out["c4_learned_closure"] = measure_c4(mlps[5])
+    out["c5_large_solve"] = measure_c5(mlps[7])
+    out["c2_forms"] = measure_c2_forms()
+    out["c1_lsw"] = measure_c1()
+    return out
+
+
+def run_one_form(name):
+    if name == "ensemble":
+        return run_forms()
+    if name == "c1":
+        return measure_c1()
+    if name == "c2":
+        return measure_c2_forms()
+    out, mlps = train_closures()
+    out[name] = measure_c4(mlps[5]) if name == "c4" else measure_c5(mlps[7])
     return out
 
 
@@ -547,9 +685,19 @@ def main():
     ap.add_argument("--impl", default="selfgpu", choices=["selfgpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the ensemble / FP32-bulk form measurements")
+    ap.add_argument("--form", choices=["c1", "c2", "c4", "c5", "ensemble"], default=None,
+                    help="run only this form's measurement and print its JSON (diagnostic mode)")
+    ap.add_argument("--cpu-table", action="store_true",
+                    help="print the CPU-baseline table of configs C1-C5 (oracle port) and exit")
     ap.add_argument("--kernel", default="persistent", choices=["persistent", "per-element"],
                     help="stage kernel: persistent bulk-copy kernel or one CTA per element group")
     args = ap.parse_args()
+    if args.cpu_table:
+        print(json.dumps(run_cpu_table()), flush=True)
+        return
+    if args.form:
+        print(json.dumps(run_one_form(args.form)), flush=True)
+        return
     from self_b200 import replicas as R
     rank, world, local_rank = R.init("gloo" if args.impl == "reference" else "nccl")
     try:
