@@ -33,7 +33,8 @@ __global__ void k_nonfinite(const double* __restrict__ q, long long n, int* flag
 }
 
 // One element's packed geometry record (geo_record_doubles<P>() doubles):
-// dsdx (4 P^2), nHat (8 P), nScale (4 P), J (P^2), then sideInfo's 20 ints.
+// dsdx (4 P^2, two planes of per-node pairs), nHat (8 P), nScale (4 P), J (P^2),
+// then sideInfo's 20 ints.
 __global__ void k_pack_geometry(const double* __restrict__ dsdx, const double* __restrict__ nHat,
                                 const double* __restrict__ nScale, const double* __restrict__ J,
                                 const int* __restrict__ sideInfo, int P, int nEl, int rec, double* __restrict__ out) {
@@ -43,8 +44,9 @@ __global__ void k_pack_geometry(const double* __restrict__ dsdx, const double* _
     const long long e = k / rec;
     int w = (int)(k - e * rec);
     double v = 0.0;
-    if (w < 4 * PP) {
-      v = dsdx[4 * PP * e + w];
+    if (w < 4 * PP) {  // plane w / (2 P^2), node (w mod 2 P^2) / 2, component w mod 2
+      const int pl = w / (2 * PP), r = w - pl * 2 * PP;
+      v = dsdx[4 * PP * e + 4 * (r >> 1) + 2 * pl + (r & 1)];
     } else if ((w -= 4 * PP) < 8 * P) {
       v = nHat[8 * P * e + w];
     } else if ((w -= 8 * P) < 4 * P) {

@@ -102,8 +102,9 @@ __device__ __forceinline__ R bm_right(const StageArgs& a, int m) {
   else return a.bMf[m + P];
 }
 
-// Doubles in one element's packed geometry record: dsdx (4 P^2), nHat (8 P),
-// nScale (4 P), J (P^2), sideInfo (20 ints = 10 doubles).
+// Doubles in one element's packed geometry record: dsdx (4 P^2, as two planes
+// of P^2 pairs: (dsdx11, dsdx21) of every node, then (dsdx12, dsdx22)), nHat
+// (8 P), nScale (4 P), J (P^2), sideInfo (20 ints = 10 doubles).
 template <int P>
 __host__ __device__ constexpr int geo_record_doubles() {
   return 5 * P * P + 12 * P + 10;

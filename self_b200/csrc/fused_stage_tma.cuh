@@ -77,18 +77,32 @@ struct TmaPlan {
   int oMats, oFlags, oSlots, oGroups, groupBytes, smemBytes;
 };
 
+// Smallest stride >= n values of `bytes` bytes whose byte size is 64 mod 128:
+// four consecutive sides then occupy alternate halves of the 32 banks.
+__host__ __device__ constexpr int side_stride(int n, int bytes) {
+  int k = n;
+  while ((k * bytes) % 128 != 64) ++k;
+  return k;
+}
+
 template <int P, class Phys, typename R>
 struct TmaTraits {
   static constexpr int PP = P * P, NV = Phys::NV, NT = Phys::NT, NF = Phys::NF;
   static constexpr int TS = trace_side_stride<P, NT, R>();
   static constexpr int TPE = (PP + 31) / 32 * 32;
   static_assert(TPE >= 4 * P, "the face phase gives each of the 4P face nodes its own thread");
-  static constexpr int kMaxGroups = 9;  // 608 threads: 96 registers each without spills (10 groups forces 80)
+  static constexpr int kMaxGroups = 9;  // 608 threads: 96 registers each (10 groups forces 80)
   static constexpr int kThreadsMax = 32 + kMaxGroups * TPE;
-  // per-group compute arrays (bulk type): the node fields of the updated
-  // solution alias the contravariant flux, then the boundary-normal flux
-  static constexpr int kU = (NF * PP > 2 * NV * PP) ? NF * PP : 2 * NV * PP;
-  static constexpr int groupBytes = (int)(((kU + 4 * NV * P) * sizeof(R) + 127) / 128 * 128);
+  // Per-group compute arrays (bulk type).  Shared-memory layouts are chosen so
+  // that a warp's accesses fall into distinct banks: arrays read along rows
+  // by one thread per row (the xi flux, the node fields of the updated
+  // solution) have rows of RS = P + 1 values; the boundary-normal flux has
+  // sides SS values apart with SS * sizeof(R) = 64 (mod 128).
+  static constexpr int RS = P + 1, PPr = P * RS;
+  static constexpr int kF = NV * PPr + NV * PP;  // xi flux [NV][P][RS], eta flux [NV][P][P]
+  static constexpr int kU = (NF * PPr > kF) ? NF * PPr : kF;  // node fields [NF][P][RS] alias the fluxes
+  static constexpr int SS = side_stride(NV * P, (int)sizeof(R));
+  static constexpr int groupBytes = (int)(((kU + 4 * SS) * sizeof(R) + 127) / 128 * 128);
 };
 
 template <int P, class Phys, typename R>
@@ -96,6 +110,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     k_fused_stage_tma(const StageArgs a, const TmaPlan pl) {
   using T = TmaTraits<P, Phys, R>;
   constexpr int NV = T::NV, NT = T::NT, NF = T::NF, PP = T::PP, TS = T::TS, TPE = T::TPE, N = P - 1;
+  constexpr int RS = T::RS, PPr = T::PPr, SS = T::SS;
   constexpr bool kLSW = (NV == 3 && !Phys::kLaggedVelocity);
   constexpr bool kSW = Phys::kLaggedVelocity;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -115,7 +130,9 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (int k = threadIdx.x; k < PP; k += blockDim.x) sdg[k] = a.dgM[k];
+  // dgMatrix transposed (sdg[i + P m] = dgM(m, i)): a warp's reads of the
+  // columns of its nodes' i (or j) are then consecutive
+  for (int k = threadIdx.x; k < PP; k += blockDim.x) sdg[k] = a.dgM[k / P + P * (k % P)];
   for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) sb[k] = a.bM[k];
   for (int k = threadIdx.x; k < P; k += blockDim.x) sqw[k] = a.qw[k];
   __syncthreads();
@@ -203,8 +220,10 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   const int barId = 1 + g;
   const bool active = t < PP;
   const int i = t % P, j = t / P;
-  R* gU = reinterpret_cast<R*>(smem + pl.oGroups + (size_t)g * pl.groupBytes);  // Fc [2][NV][PP], later fld [NF][PP]
-  R* gfb = gU + T::kU;                                                            // [4][NV][P]
+  R* gU = reinterpret_cast<R*>(smem + pl.oGroups + (size_t)g * pl.groupBytes);  // fluxes, later node fields
+  R* gF1 = gU + NV * PPr;                                                         // eta flux [NV][P][P]
+  R* gfb = gU + T::kU;                                                            // [4][SS]: [NV][P] per side
+  const int tr = i + RS * j;                                                      // this node in a padded array
   R* trOut = reinterpret_cast<R*>(a.trOut);
 
   for (long long jj = 0;; ++jj) {
@@ -230,20 +249,10 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       break;
     }
     const int* ssi = reinterpret_cast<const int*>(sl + pl.oSi);
-
-    // ---- A: solution (kept in registers), flux auxiliaries, contravariant flux
-    double qv[NV], Jij = 1.0;
-    R f[NF];
-    double na[3] = {0.0, 0.0, 0.0};
-    if (active) {
-      Jij = reinterpret_cast<const double*>(sl + pl.oJ)[t];  // read before the buffer is released
-      const double* sq = reinterpret_cast<const double*>(sl + pl.oQ);
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        qv[v] = sq[t + PP * v];
-        f[v] = (R)qv[v];
-      }
-      Phys::template node_flux<R>(f, a);
+    const double* sq = reinterpret_cast<const double*>(sl + pl.oQ);
+    // node auxiliaries of this element, read from the buffer where they are used
+    auto node_aux = [&](double na[3]) {
+      na[0] = na[1] = na[2] = 0.0;
       if constexpr (kLSW) {
         na[0] = reinterpret_cast<const double*>(sl + pl.oX[0])[t];
         if (pl.oX[2] >= 0) na[1] = reinterpret_cast<const double*>(sl + pl.oX[2])[t];
@@ -261,10 +270,24 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         }
         if (pl.oX[1] >= 0) na[2] = reinterpret_cast<const double*>(sl + pl.oX[1])[t];
       }
+    };
+
+    // ---- A: flux auxiliaries, contravariant flux.  The buffer stays valid
+    // until the end of phase D, so the solution, J and the node auxiliaries
+    // are read again where they are needed instead of living in registers
+    // across the face phase.
+    R f[NF];
+    if (active) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) f[v] = (R)sq[t + PP * v];
+      Phys::template node_flux<R>(f, a);
+      double na[3];
+      node_aux(na);
       R Fx[NV], Fy[NV];
       Phys::template flux<R>(f, na, a, Fx, Fy);
-      const double2* gp = reinterpret_cast<const double2*>(sl + pl.oDsdx) + 2 * t;
-      const double2 c1 = gp[0], c2 = gp[1];
+      // dsdx planes: (dsdx11, dsdx21) of every node, then (dsdx12, dsdx22)
+      const double2* gp = reinterpret_cast<const double2*>(sl + pl.oDsdx);
+      const double2 c1 = gp[t], c2 = gp[PP + t];
       R F0[NV], F1[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
@@ -275,8 +298,8 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         if (a.av) av_volume_add<P, R>(a, t, e, F0, F1);
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        gU[v * PP + t] = F0[v];
-        gU[(NV + v) * PP + t] = F1[v];
+        gU[v * PPr + tr] = F0[v];
+        gF1[v * PP + t] = F1[v];
       }
     }
 
@@ -338,24 +361,27 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       if constexpr (NV == 4)
         if (a.av) av_face_add<P, R>(a, s1, ii, e, ssi + 5 * s1, nh.x, nh.y, ns, out);
 #pragma unroll
-      for (int v = 0; v < NV; ++v) gfb[(s1 * NV + v) * P + ii] = out[v];
+      for (int v = 0; v < NV; ++v) gfb[s1 * SS + v * P + ii] = out[v];
     }
-    named_bar(barId, TPE);  // flux and face values ready; this buffer is no longer read
-    if (t == 0) mbar_arrive(&empty[2 * g + buf]);
+    named_bar(barId, TPE);  // flux and face values ready
 
     // ---- D: weak divergence + lift, 1/J, source, RK update
-    double dsdt[NV];
+    double dsdt[NV], qv[NV];
     if (active) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) qv[v] = sq[t + PP * v];
+      const double Jij = reinterpret_cast<const double*>(sl + pl.oJ)[t];
       // sources in FP64 in every form (well-balanced topography / gravity terms)
-      double Src[NV];
+      double Src[NV], na[3];
+      node_aux(na);
       Phys::template source<double>(qv, na, a, Src);
       const R wi = (R)sqw[i], wj = (R)sqw[j];
       // dgMatrix columns of this node's i and j, shared by the four variables
       R dgi[P], dgj[P];
 #pragma unroll
       for (int m = 0; m < P; ++m) {
-        dgi[m] = (R)sdg[m + P * i];
-        dgj[m] = (R)sdg[m + P * j];
+        dgi[m] = (R)sdg[i + P * m];
+        dgj[m] = (R)sdg[j + P * m];
       }
       // the four variables' sums advance together (independent dependency chains);
       // each keeps the reference's order over m
@@ -366,22 +392,23 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       for (int m = 0; m < P; ++m) {
 #pragma unroll
         for (int v = 0; v < NV; ++v)
-          d[v] = d[v] + dgi[m] * gU[v * PP + m + P * j] + dgj[m] * gU[(NV + v) * PP + i + P * m];
+          d[v] = d[v] + dgi[m] * gU[v * PPr + m + RS * j] + dgj[m] * gF1[v * PP + i + P * m];
       }
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        const R dv = d[v] + ((R)sb[i + P] * gfb[(1 * NV + v) * P + j] + (R)sb[i] * gfb[(3 * NV + v) * P + j]) / wi +
-                     ((R)sb[j + P] * gfb[(2 * NV + v) * P + i] + (R)sb[j] * gfb[(0 * NV + v) * P + i]) / wj;
+        const R dv = d[v] + ((R)sb[i + P] * gfb[1 * SS + v * P + j] + (R)sb[i] * gfb[3 * SS + v * P + j]) / wi +
+                     ((R)sb[j + P] * gfb[2 * SS + v * P + i] + (R)sb[j] * gfb[0 * SS + v * P + i]) / wj;
         dsdt[v] = Src[v] - (double)dv / Jij;
       }
     }
+    named_bar(barId, TPE);  // every thread is done reading the flux array and the buffer
+    if (t == 0) mbar_arrive(&empty[2 * g + buf]);
     if (!rk) {
       if (active)
 #pragma unroll
         for (int v = 0; v < NV; ++v) a.dSdt[t + (size_t)PP * (v + NV * (size_t)e)] = dsdt[v];
-      continue;  // the next element's post-wait barrier orders the reuse of the flux array
+      continue;
     }
-    named_bar(barId, TPE);  // every thread is done reading the flux array
     if (active) {
       const double gdt = a.dtElem ? a.rk_g * a.dtElem[e] : a.rk_gdt;
 #pragma unroll
@@ -395,7 +422,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       }
       Phys::template node<R>(f, a);
 #pragma unroll
-      for (int v = 0; v < NF; ++v) gU[v * PP + t] = f[v];
+      for (int v = 0; v < NF; ++v) gU[v * PPr + tr] = f[v];
     }
     named_bar(barId, TPE);
 
@@ -407,8 +434,8 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       R* o = trOut + (size_t)4 * TS * e;
       for (int kk = t; kk < 2 * NT * P; kk += TPE) {
         const int fi = kk / (2 * P), rem = kk - fi * 2 * P, row = rem / P, l = rem - row * P;
-        const R* fv = gU + fi * PP + (row ? P * l : l);
-        const int stride = row ? 1 : P;
+        const R* fv = gU + fi * PPr + (row ? RS * l : l);
+        const int stride = row ? 1 : RS;
         R lo = (R)0, hi = (R)0;
 #pragma unroll
         for (int m = 0; m < P; ++m) {
