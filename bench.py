@@ -91,16 +91,50 @@ def initial_state(x):
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region.
+
+    An in-process NVML reader thread (every 10 ms, so that even a timed region
+    of a few hundred milliseconds has samples); `nvidia-smi -lms 200` when NVML
+    cannot be loaded.  Only reads the GPU's state."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
-        self.index, self.proc = index, None
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.index, self.proc, self.thread = index, None, None
+        self.sm, self.mx, self.reasons = [], None, set()
+        self.f = None
+
+    def _nvml_loop(self, nv, h, bits):
+        while not self.stop.is_set():
+            try:
+                self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for nm, b in zip(self.NAMES, bits):
+                    if r & b:
+                        self.reasons.add(nm)
+            except Exception:
+                pass
+            self.stop.wait(0.01)
 
     def __enter__(self):
+        try:
+            import threading
+            import pynvml as nv
+            nv.nvmlInit()
+            idx = str(self.index)
+            h = nv.nvmlDeviceGetHandleByUUID(idx) if idx.startswith("GPU-") else nv.nvmlDeviceGetHandleByIndex(int(idx))
+            self.mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h, bits), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
@@ -110,30 +144,35 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
+        if self.thread:
+            self.stop.set()
+            self.thread.join()
         if self.proc:
             self.proc.terminate()
             self.proc.wait()
 
     def summary(self):
-        self.f.flush()
-        self.f.seek(0)
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.f:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        os.unlink(self.f.name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if self.f is not None:
+            self.f.flush()
+            self.f.seek(0)
+            for line in self.f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    self.sm.append(float(parts[1]))
+                    self.mx = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(self.NAMES, parts[5:9]):
+                    if v.lower() == "active":
+                        self.reasons.add(nm)
+            os.unlink(self.f.name)
+            self.f = None
+        sm = self.sm
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.mx,
+                "reasons": sorted(self.reasons), "samples": len(sm),
+                "source": "nvml" if self.thread is not None else "nvidia-smi"}
 
 
 def cpu_baseline(seconds=12.0, max_steps=STEPS_PER_SOLVE):

@@ -93,16 +93,29 @@ struct TmaTraits {
   static_assert(TPE >= 4 * P, "the face phase gives each of the 4P face nodes its own thread");
   static constexpr int kMaxGroups = 9;  // 608 threads: 96 registers each (10 groups forces 80)
   static constexpr int kThreadsMax = 32 + kMaxGroups * TPE;
-  // Per-group compute arrays (bulk type).  Shared-memory layouts are chosen so
-  // that a warp's accesses fall into distinct banks: arrays read along rows
-  // by one thread per row (the xi flux, the node fields of the updated
-  // solution) have rows of RS = P + 1 values; the boundary-normal flux has
-  // sides SS values apart with SS * sizeof(R) = 64 (mod 128).
-  static constexpr int RS = P + 1, PPr = P * RS;
-  static constexpr int kF = NV * PPr + NV * PP;  // xi flux [NV][P][RS], eta flux [NV][P][P]
-  static constexpr int kU = (NF * PPr > kF) ? NF * PPr : kF;  // node fields [NF][P][RS] alias the fluxes
+  // Per-group compute arrays (bulk type), laid out for conflict-free shared
+  // accesses.  A 64-bit shared access is served per half-warp: two threads of
+  // a half-warp that touch different words of one bank pair (8-byte word
+  // index mod 16) cost an extra pass.
+  //  * contravariant fluxes [2][NV][P][P]: a half-warp holds rows j and j + 1.
+  //  * node fields of the updated solution, read one line per thread by the
+  //    trace tasks: field stride FS = 8 (mod 16) and, for P = 8, the column
+  //    index XOR-swizzled per (field, row) so that the column lines and the
+  //    row lines of two fields fall into distinct bank pairs; other P pad
+  //    rows to P + 1.
+  //  * boundary-normal flux [4][SS]: sides SS values apart, SS * sizeof(R) =
+  //    64 (mod 128).
+  static constexpr bool kSwz = (P == 8);
+  static constexpr int RS = kSwz ? P : P + 1;
+  static constexpr int FS = kSwz ? PP + 8 : P * RS;
+  static constexpr int kU = (NF * FS > 2 * NV * PP) ? NF * FS : 2 * NV * PP;  // node fields alias the fluxes
   static constexpr int SS = side_stride(NV * P, (int)sizeof(R));
   static constexpr int groupBytes = (int)(((kU + 4 * SS) * sizeof(R) + 127) / 128 * 128);
+  // offset of node (i, j) in field f's block of the node-field array
+  __device__ __forceinline__ static int nf(int f, int i, int j) {
+    if constexpr (kSwz) return P * j + (i ^ (((j >> 1) ^ (4 * (f & 1))) & (P - 1)));
+    else return RS * j + i;
+  }
 };
 
 template <int P, class Phys, typename R>
@@ -110,7 +123,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     k_fused_stage_tma(const StageArgs a, const TmaPlan pl) {
   using T = TmaTraits<P, Phys, R>;
   constexpr int NV = T::NV, NT = T::NT, NF = T::NF, PP = T::PP, TS = T::TS, TPE = T::TPE, N = P - 1;
-  constexpr int RS = T::RS, PPr = T::PPr, SS = T::SS;
+  constexpr int FS = T::FS, SS = T::SS;
   constexpr bool kLSW = (NV == 3 && !Phys::kLaggedVelocity);
   constexpr bool kSW = Phys::kLaggedVelocity;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -146,7 +159,6 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     // ------------------------------------------------------------ producer
     const int lane = threadIdx.x & 31;
     bool abort = false;
-    long long issued = 0;
     if (lane == 0) {
       const R* trIn = reinterpret_cast<const R*>(a.trIn);
       const R* vIn = reinterpret_cast<const R*>(a.velIn);
@@ -166,21 +178,12 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       }
       uint32_t bytes = qb + gb + ob + xb[0] + xb[1] + xb[2] + xb[3] + xb[4];
       if constexpr (kSW) bytes += 8 * P * sizeof(R);
-      for (long long k = 0; k < nMine; ++k) {
-        const int g = (int)(k % C);
-        const long long jj = k / C;
-        const int buf = (int)(jj & 1);
-        const uint32_t par = (uint32_t)((jj >> 1) & 1);
-        if (!mbar_wait(&empty[2 * g + buf], par ^ 1u, a.waitCycles)) {
-          abort = true;
-          break;
-        }
+      auto issue = [&](long long k, int g, int buf) {
         const long long e = blockIdx.x + k * gridDim.x;
         unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
         uint64_t* bar = &full[2 * g + buf];
         mbar_arrive_expect_tx(bar, bytes);
-        issued = k + 1;
-        if (a.debugStarve && blockIdx.x == 0 && k == 0) continue;
+        if (a.debugStarve && blockIdx.x == 0 && k == 0) return;
         bulk_g2s(sl + pl.oQ, a.q + (size_t)e * NV * PP, qb, bar);
         bulk_g2s(sl + pl.oDsdx, a.geo + (size_t)e * geo_record_doubles<P>(), gb, bar);
         bulk_g2s(sl + pl.oOwn, trIn + (size_t)4 * TS * e, ob, bar);
@@ -198,15 +201,43 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
           if (xb[2])
             for (int x = 2; x < 5; ++x) bulk_g2s(sl + pl.oX[x], a.fld[x] + (size_t)e * 16 * P, xb[x], bar);
         }
+      };
+      // Group g consumes the CTA's elements g, g + C, g + 2C, ... in its two
+      // buffers.  The groups are served round-robin as their buffers free up,
+      // so a group that is behind does not hold back the copies of the others.
+      int* nextJ = const_cast<int*>(gflag) + C;  // per group: local index of the next element to issue
+      for (int g = 0; g < C; ++g) nextJ[g] = 0;
+      long long remaining = nMine, idle0 = clock64();
+      while (remaining > 0) {
+        bool progress = false;
+        for (int g = 0; g < C; ++g) {
+          const int jj = nextJ[g];
+          const long long k = g + (long long)jj * C;
+          if (k >= nMine) continue;
+          const int buf = jj & 1;
+          if (!mbar_try_wait(&empty[2 * g + buf], (uint32_t)((jj >> 1) & 1) ^ 1u)) continue;
+          issue(k, g, buf);
+          nextJ[g] = jj + 1;
+          --remaining;
+          progress = true;
+        }
+        if (progress) {
+          idle0 = clock64();
+        } else {
+          if (clock64() - idle0 > a.waitCycles) {
+            abort = true;
+            break;
+          }
+          __nanosleep(32);
+        }
       }
       if (abort) {
         if (a.err) atomicExch(a.err, 1);
         // Wait (bounded) for the copies already issued into buffers no consumer
         // will read any more, so none is in flight when the CTA exits.
-        for (long long k = (issued > 2 * C ? issued - 2 * C : 0); k < issued; ++k) {
-          const int g = (int)(k % C);
-          const long long jj = k / C;
-          mbar_wait(&full[2 * g + (int)(jj & 1)], (uint32_t)((jj >> 1) & 1), a.waitCycles);
+        for (int g = 0; g < C; ++g) {
+          for (int jj = (nextJ[g] > 2 ? nextJ[g] - 2 : 0); jj < nextJ[g]; ++jj)
+            mbar_wait(&full[2 * g + (jj & 1)], (uint32_t)((jj >> 1) & 1), a.waitCycles);
         }
       }
     }
@@ -221,9 +252,8 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   const bool active = t < PP;
   const int i = t % P, j = t / P;
   R* gU = reinterpret_cast<R*>(smem + pl.oGroups + (size_t)g * pl.groupBytes);  // fluxes, later node fields
-  R* gF1 = gU + NV * PPr;                                                         // eta flux [NV][P][P]
+  R* gF1 = gU + NV * PP;                                                          // eta flux [NV][P][P]
   R* gfb = gU + T::kU;                                                            // [4][SS]: [NV][P] per side
-  const int tr = i + RS * j;                                                      // this node in a padded array
   R* trOut = reinterpret_cast<R*>(a.trOut);
 
   for (long long jj = 0;; ++jj) {
@@ -298,7 +328,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         if (a.av) av_volume_add<P, R>(a, t, e, F0, F1);
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        gU[v * PPr + tr] = F0[v];
+        gU[v * PP + t] = F0[v];
         gF1[v * PP + t] = F1[v];
       }
     }
@@ -392,7 +422,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       for (int m = 0; m < P; ++m) {
 #pragma unroll
         for (int v = 0; v < NV; ++v)
-          d[v] = d[v] + dgi[m] * gU[v * PPr + m + RS * j] + dgj[m] * gF1[v * PP + i + P * m];
+          d[v] = d[v] + dgi[m] * gU[v * PP + m + P * j] + dgj[m] * gF1[v * PP + i + P * m];
       }
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
@@ -422,7 +452,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       }
       Phys::template node<R>(f, a);
 #pragma unroll
-      for (int v = 0; v < NF; ++v) gU[v * PPr + tr] = f[v];
+      for (int v = 0; v < NF; ++v) gU[v * FS + T::nf(v, i, j)] = f[v];
     }
     named_bar(barId, TPE);
 
@@ -430,16 +460,22 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     // (field, line, orientation) reads the line's P values once and forms both
     // of its end traces (BoundaryInterp, src/SELF_Lagrange.f90:2241-2270):
     // column l gives S (side 0) and N (side 2), row l gives W (3) and E (1).
+    // Tasks are numbered by field pair, orientation, field, line, so that for
+    // P = 8 a half-warp reads the column lines (or the row lines) of two fields.
     {
       R* o = trOut + (size_t)4 * TS * e;
-      for (int kk = t; kk < 2 * NT * P; kk += TPE) {
-        const int fi = kk / (2 * P), rem = kk - fi * 2 * P, row = rem / P, l = rem - row * P;
-        const R* fv = gU + fi * PPr + (row ? RS * l : l);
-        const int stride = row ? 1 : RS;
+      constexpr int NTp = (NT + 1) / 2 * 2;
+      // the face threads (t < 4P, the first warp) start one warp later, so the
+      // second warp takes the last, partial round
+      for (int kk = (t + 32) % TPE; kk < 2 * NTp * P; kk += TPE) {
+        const int fp = kk / (4 * P), r = kk - fp * 4 * P, row = r / (2 * P), r2 = r - row * 2 * P, fs = r2 / P;
+        const int l = r2 - fs * P, fi = 2 * fp + fs;
+        if (fi >= NT) continue;
+        const R* fv = gU + fi * FS;
         R lo = (R)0, hi = (R)0;
 #pragma unroll
         for (int m = 0; m < P; ++m) {
-          const R x = fv[stride * m];
+          const R x = fv[row ? T::nf(fi, m, l) : T::nf(fi, l, m)];
           lo = lo + bm_left<R>(a, m) * x;
           hi = hi + bm_right<R, P>(a, m) * x;
         }
@@ -499,7 +535,7 @@ inline bool make_tma_plan(const StageArgs& a, int smemLimit, TmaPlan& pl, int ma
     const int oMats = s;
     s += (PP + 3 * P) * 8;
     const int oFlags = s;
-    s += C * 4;
+    s += 2 * C * 4;  // consumer flags, producer counters
     s = (s + 127) / 128 * 128;
     const int oSlots = s;
     s += 2 * C * pl.slotBytes;
