@@ -111,6 +111,18 @@ struct TmaTraits {
   static constexpr int kU = (NF * FS > 2 * NV * PP) ? NF * FS : 2 * NV * PP;  // node fields alias the fluxes
   static constexpr int SS = side_stride(NV * P, (int)sizeof(R));
   static constexpr int groupBytes = (int)(((kU + 4 * SS) * sizeof(R) + 127) / 128 * 128);
+  // Weak-divergence volume sums: one thread per 2x2 block of nodes and pair
+  // of variables, all in one warp.  The xi flux rows are stored with their
+  // value pairs XOR-swizzled per row pair (P/2 a power of two), so that the
+  // paired loads of a quarter-warp fall into distinct banks.
+  static constexpr int HB = P / 2, NVP = (NV + 1) / 2, NB = HB * HB * NVP;
+  static_assert(NB <= 32, "the divergence blocks fit one warp");
+  static constexpr bool kSwzF = (HB & (HB - 1)) == 0;
+  // position of value m in row j of the xi flux
+  __device__ __forceinline__ static int f0pos(int m, int j) {
+    if constexpr (kSwzF) return 2 * ((m >> 1) ^ ((j >> 1) & (HB - 1))) + (m & 1);
+    else return m;
+  }
   // offset of node (i, j) in field f's block of the node-field array
   __device__ __forceinline__ static int nf(int f, int i, int j) {
     if constexpr (kSwz) return P * j + (i ^ (((j >> 1) ^ (4 * (f & 1))) & (P - 1)));
@@ -251,6 +263,10 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   const int barId = 1 + g;
   const bool active = t < PP;
   const int i = t % P, j = t / P;
+  // Which warp of the group runs the face phase (the other one sums the
+  // divergence meanwhile): alternated in pairs of groups so that both kinds
+  // of work spread over the SM's four schedulers (warp w runs on w mod 4).
+  const int faceWarp = (TPE >= 64) ? ((g >> 1) & 1) : 0;
   R* gU = reinterpret_cast<R*>(smem + pl.oGroups + (size_t)g * pl.groupBytes);  // fluxes, later node fields
   R* gF1 = gU + NV * PP;                                                          // eta flux [NV][P][P]
   R* gfb = gU + T::kU;                                                            // [4][SS]: [NV][P] per side
@@ -263,15 +279,6 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     const int buf = (int)(jj & 1);
     const uint32_t par = (uint32_t)((jj >> 1) & 1);
     const unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
-    // RK register straight from global memory; it is first used after the
-    // face phase, which hides the latency.
-    double Gv[NV];
-    if (active) {
-      if (rk) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) Gv[v] = a.G[t + (size_t)PP * (v + NV * (size_t)e)];
-      }
-    }
     if (t == 0) gflag[g] = mbar_wait(&full[2 * g + buf], par, a.waitCycles) ? 1 : 0;
     named_bar(barId, TPE);
     if (!gflag[g]) {
@@ -328,14 +335,88 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         if (a.av) av_volume_add<P, R>(a, t, e, F0, F1);
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        gU[v * PP + t] = F0[v];
+        gU[v * PP + P * j + T::f0pos(i, j)] = F0[v];
         gF1[v * PP + t] = F1[v];
+      }
+    }
+    named_bar(barId, TPE);  // contravariant fluxes ready
+
+    // ---- B (alongside the face phase C, in the group's other warp): weak-
+    // divergence volume sums, the reference's order per node and variable
+    // (VectorDGDivergence_2D, src/SELF_Lagrange.f90):
+    //   d = 0;  for m ascending: d = (d + dgM(m,i) F0(m,j)) + dgM(m,j) F1(i,m).
+    // A thread sums a 2x2 block of nodes for two variables, so every loaded
+    // flux pair and dgMatrix pair serves two nodes.  The sums replace the xi
+    // flux in shared memory ([NV][P^2], node-major) once the warp has read it.
+    if (TPE < 64 || (t >> 5) != faceWarp) {
+      using R2 = typename std::conditional<sizeof(R) == 8, double2, float2>::type;
+      constexpr int HB = T::HB;
+      const int tb = t & 31;
+      const bool on = tb < T::NB;
+      const int vp = tb / (HB * HB), rem = tb - vp * (HB * HB), bj = rem / HB, bi = rem - bj * HB;
+      const int v0 = 2 * vp;
+      const bool two = v0 + 1 < NV;
+      R acc[2][2][2];  // [variable of the pair][row offset r (j)][column offset c (i)]
+#pragma unroll
+      for (int vv = 0; vv < 2; ++vv)
+#pragma unroll
+        for (int r = 0; r < 2; ++r) acc[vv][r][0] = acc[vv][r][1] = (R)0;
+      if (on) {
+        const double2* sdg2 = reinterpret_cast<const double2*>(sdg);
+#pragma unroll
+        for (int mp = 0; mp < HB; ++mp) {
+          R f0[2][2][2];  // [vv][r][k]: F0(2 mp + k, 2 bj + r)
+          R f1[2][2][2];  // [vv][k][c]: F1(2 bi + c, 2 mp + k)
+#pragma unroll
+          for (int vv = 0; vv < 2; ++vv) {
+            const int v = (vv == 0 || two) ? v0 + vv : v0;
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+              const int row = 2 * bj + r;
+              const R2 x = reinterpret_cast<const R2*>(gU + v * PP + P * row)[T::f0pos(2 * mp, row) >> 1];
+              f0[vv][r][0] = x.x;
+              f0[vv][r][1] = x.y;
+            }
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+              const R2 x = reinterpret_cast<const R2*>(gF1 + v * PP + P * (2 * mp + k))[bi];
+              f1[vv][k][0] = x.x;
+              f1[vv][k][1] = x.y;
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            const int m = 2 * mp + k;
+            const double2 dI = sdg2[bi + HB * m], dJ = sdg2[bj + HB * m];
+            const R gi[2] = {(R)dI.x, (R)dI.y}, gj[2] = {(R)dJ.x, (R)dJ.y};
+#pragma unroll
+            for (int vv = 0; vv < 2; ++vv)
+#pragma unroll
+              for (int r = 0; r < 2; ++r)
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+                  acc[vv][r][c] = acc[vv][r][c] + gi[c] * f0[vv][r][k] + gj[r] * f1[vv][k][c];
+          }
+        }
+      }
+      __syncwarp();  // the warp has read the xi flux
+      if (on) {
+#pragma unroll
+        for (int vv = 0; vv < 2; ++vv)
+          if (vv == 0 || two)
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+              R2 x;
+              x.x = acc[vv][r][0];
+              x.y = acc[vv][r][1];
+              reinterpret_cast<R2*>(gU + (v0 + vv) * PP + P * (2 * bj + r))[bi] = x;
+            }
       }
     }
 
     // ---- C: faces; own traces of this stage's solution come from the cache
-    if (t < 4 * P) {
-      const int s1 = t / P, ii = t % P;
+    if ((t >> 5) == faceWarp && (t & 31) < 4 * P) {
+      const int s1 = (t & 31) / P, ii = (t & 31) % P;
       const int bcid = ssi[5 * s1 + 4];
       const bool physical = (bcid != 0) && (ssi[5 * s1 + 2] == 0);
       const int flip = ssi[5 * s1 + 3] % 10;
@@ -396,8 +477,12 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     named_bar(barId, TPE);  // flux and face values ready
 
     // ---- D: weak divergence + lift, 1/J, source, RK update
-    double dsdt[NV], qv[NV];
+    double dsdt[NV], qv[NV], Gv[NV];
     if (active) {
+      if (rk) {  // RK register from global memory; the lift below hides the latency
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Gv[v] = a.G[t + (size_t)PP * (v + NV * (size_t)e)];
+      }
 #pragma unroll
       for (int v = 0; v < NV; ++v) qv[v] = sq[t + PP * v];
       const double Jij = reinterpret_cast<const double*>(sl + pl.oJ)[t];
@@ -406,24 +491,9 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       node_aux(na);
       Phys::template source<double>(qv, na, a, Src);
       const R wi = (R)sqw[i], wj = (R)sqw[j];
-      // dgMatrix columns of this node's i and j, shared by the four variables
-      R dgi[P], dgj[P];
+      R d[NV];  // volume sums from phase B
 #pragma unroll
-      for (int m = 0; m < P; ++m) {
-        dgi[m] = (R)sdg[i + P * m];
-        dgj[m] = (R)sdg[j + P * m];
-      }
-      // the four variables' sums advance together (independent dependency chains);
-      // each keeps the reference's order over m
-      R d[NV];
-#pragma unroll
-      for (int v = 0; v < NV; ++v) d[v] = (R)0;
-#pragma unroll
-      for (int m = 0; m < P; ++m) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v)
-          d[v] = d[v] + dgi[m] * gU[v * PP + m + P * j] + dgj[m] * gF1[v * PP + i + P * m];
-      }
+      for (int v = 0; v < NV; ++v) d[v] = gU[v * PP + t];
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
         const R dv = d[v] + ((R)sb[i + P] * gfb[1 * SS + v * P + j] + (R)sb[i] * gfb[3 * SS + v * P + j]) / wi +
@@ -465,9 +535,9 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     {
       R* o = trOut + (size_t)4 * TS * e;
       constexpr int NTp = (NT + 1) / 2 * 2;
-      // the face threads (t < 4P, the first warp) start one warp later, so the
-      // second warp takes the last, partial round
-      for (int kk = (t + 32) % TPE; kk < 2 * NTp * P; kk += TPE) {
+      // the face warp starts one warp later, so the other warp takes the
+      // last, partial round
+      for (int kk = faceWarp ? t : (t + 32) % TPE; kk < 2 * NTp * P; kk += TPE) {
         const int fp = kk / (4 * P), r = kk - fp * 4 * P, row = r / (2 * P), r2 = r - row * 2 * P, fs = r2 / P;
         const int l = r2 - fs * P, fi = 2 * fp + fs;
         if (fi >= NT) continue;
