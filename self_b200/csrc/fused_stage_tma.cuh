@@ -1,21 +1,23 @@
-// Persistent, warp-specialised variant of the fused stage kernel.
+// Persistent variant of the fused stage kernel.
 //
-// One CTA per SM.  Warp 0 is the producer: for every element the CTA owns it
-// issues 1-D bulk asynchronous copies (cp.async.bulk, the non-tensor TMA path)
-// of the element's contiguous blocks -- solution, the engine's packed
-// geometry record (dsdx, nHat, nScale, J, sideInfo), its own face traces and
-// the model fields -- into a shared-memory buffer whose mbarrier counts the
-// bytes in.  Bulk copies are issued one at a time by one lane: the number of
-// copy requests per element, not their bytes, limits the producer, so the
-// per-element pieces that live in separate arrays are packed into one record
-// at set-up.  The remaining warps form C consumer groups of TPE threads (one
-// thread per node); each group owns two buffers, so the copies for its next
-// element are in flight while it computes the current one.  The face threads
-// load the neighbours' trace values themselves (coalesced plain loads).
+// One CTA per SM, made of C consumer groups of TPE threads (one thread per
+// node).  A group works through the CTA's elements g, g + C, g + 2C, ... and
+// owns two shared-memory buffers: for every element its thread 0 issues 1-D
+// bulk asynchronous copies (cp.async.bulk, the non-tensor TMA path) of the
+// element's contiguous blocks -- solution, the engine's packed geometry record
+// (dsdx, nHat, nScale, J, sideInfo), its own face traces and the model fields
+// -- into a buffer whose mbarrier counts the bytes in, two elements ahead: the
+// copies for element jj + 2 go out as soon as element jj has released its
+// buffer.  The number of copy requests per element, not their bytes, is what
+// costs, so the per-element pieces that live in separate arrays are packed
+// into one record at set-up.  The face threads load the neighbours' trace
+// values themselves (coalesced plain loads).  With no separate producer warp,
+// ten groups of two warps fill the SM's four schedulers with five warps each
+// at 96 registers per thread.
 //
-// Every wait is bounded (StageArgs::waitCycles): on timeout the kernel records
-// an error word, stops issuing copies, waits (again bounded) for copies it has
-// already issued and returns; the host reports SELFGPU_ERR_TIMEOUT.
+// Every wait is bounded (StageArgs::waitCycles): on timeout the group records
+// an error word, waits (again bounded) for its other copy in flight and
+// returns; the host reports SELFGPU_ERR_TIMEOUT.
 //
 // Requires an even P (all per-element block sizes are then multiples of 16
 // bytes) and 16-byte aligned base pointers; the engine falls back to
@@ -91,8 +93,8 @@ struct TmaTraits {
   static constexpr int TS = trace_side_stride<P, NT, R>();
   static constexpr int TPE = (PP + 31) / 32 * 32;
   static_assert(TPE >= 4 * P, "the face phase gives each of the 4P face nodes its own thread");
-  static constexpr int kMaxGroups = 9;  // 608 threads: 96 registers each (10 groups forces 80)
-  static constexpr int kThreadsMax = 32 + kMaxGroups * TPE;
+  static constexpr int kMaxGroups = 10;  // 640 threads: five warps per scheduler at 96 registers
+  static constexpr int kThreadsMax = kMaxGroups * TPE;
   // Per-group compute arrays (bulk type), laid out for conflict-free shared
   // accesses.  A 64-bit shared access is served per half-warp: two threads of
   // a half-warp that touch different words of one bank pair (8-byte word
@@ -141,7 +143,6 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   extern __shared__ __align__(128) unsigned char smem[];
   const int C = pl.groups;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
-  uint64_t* empty = full + 2 * C;
   double* sdg = reinterpret_cast<double*>(smem + pl.oMats);
   double* sb = sdg + PP;
   double* sqw = sb + 2 * P;
@@ -149,10 +150,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   unsigned char* slots = smem + pl.oSlots;
 
   if (threadIdx.x == 0) {
-    for (int k = 0; k < 2 * C; ++k) {
-      mbar_init(&full[k], 1);
-      mbar_init(&empty[k], 1);
-    }
+    for (int k = 0; k < 2 * C; ++k) mbar_init(&full[k], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   // dgMatrix transposed (sdg[i + P m] = dgM(m, i)): a warp's reads of the
@@ -164,102 +162,64 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
 
   const long long nMine =
       (long long)blockIdx.x < a.nEl ? ((long long)a.nEl - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
-  const int warp = threadIdx.x >> 5;
   const bool rk = (a.mode == MODE_RK);
+  const int g = threadIdx.x / TPE;
+  const int t = threadIdx.x % TPE;
+  if (g >= C) return;
 
-  if (warp == 0) {
-    // ------------------------------------------------------------ producer
-    const int lane = threadIdx.x & 31;
-    bool abort = false;
-    if (lane == 0) {
-      const R* trIn = reinterpret_cast<const R*>(a.trIn);
-      const R* vIn = reinterpret_cast<const R*>(a.velIn);
-      const uint32_t qb = NV * PP * 8, gb = geo_record_doubles<P>() * 8, ob = 4 * TS * sizeof(R);
-      uint32_t xb[5] = {0, 0, 0, 0, 0};
-      if constexpr (kLSW) {
-        xb[0] = PP * 8;
-        xb[1] = 4 * P * 8;
-        xb[2] = a.fld[2] ? PP * 8 : 0;
-      } else if constexpr (kSW) {
-        xb[0] = a.fld[0] ? 4 * P * 8 : 0;
-        xb[1] = a.fld[1] ? 2 * PP * 8 : 0;
-      } else {
-        xb[0] = a.fld[0] ? 2 * PP * 8 : 0;
-        xb[1] = a.fld[1] ? PP * 8 : 0;
-        xb[2] = xb[3] = xb[4] = a.fld[2] ? 16 * P * 8 : 0;
-      }
-      uint32_t bytes = qb + gb + ob + xb[0] + xb[1] + xb[2] + xb[3] + xb[4];
-      if constexpr (kSW) bytes += 8 * P * sizeof(R);
-      auto issue = [&](long long k, int g, int buf) {
-        const long long e = blockIdx.x + k * gridDim.x;
-        unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
-        uint64_t* bar = &full[2 * g + buf];
-        mbar_arrive_expect_tx(bar, bytes);
-        if (a.debugStarve && blockIdx.x == 0 && k == 0) return;
-        bulk_g2s(sl + pl.oQ, a.q + (size_t)e * NV * PP, qb, bar);
-        bulk_g2s(sl + pl.oDsdx, a.geo + (size_t)e * geo_record_doubles<P>(), gb, bar);
-        bulk_g2s(sl + pl.oOwn, trIn + (size_t)4 * TS * e, ob, bar);
-        if constexpr (kSW) bulk_g2s(sl + pl.oVelOwn, vIn + (size_t)e * 8 * P, 8 * P * sizeof(R), bar);
-        if constexpr (kLSW) {
-          bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * PP, xb[0], bar);
-          bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 4 * P, xb[1], bar);
-          if (xb[2]) bulk_g2s(sl + pl.oX[2], a.fld[2] + (size_t)e * PP, xb[2], bar);
-        } else if constexpr (kSW) {
-          if (xb[0]) bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * 4 * P, xb[0], bar);
-          if (xb[1]) bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 2 * PP, xb[1], bar);
-        } else {
-          if (xb[0]) bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * 4 * PP, xb[0], bar);
-          if (xb[1]) bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 2 * PP + PP, xb[1], bar);
-          if (xb[2])
-            for (int x = 2; x < 5; ++x) bulk_g2s(sl + pl.oX[x], a.fld[x] + (size_t)e * 16 * P, xb[x], bar);
-        }
-      };
-      // Group g consumes the CTA's elements g, g + C, g + 2C, ... in its two
-      // buffers.  The groups are served round-robin as their buffers free up,
-      // so a group that is behind does not hold back the copies of the others.
-      int* nextJ = const_cast<int*>(gflag) + C;  // per group: local index of the next element to issue
-      for (int g = 0; g < C; ++g) nextJ[g] = 0;
-      long long remaining = nMine, idle0 = clock64();
-      while (remaining > 0) {
-        bool progress = false;
-        for (int g = 0; g < C; ++g) {
-          const int jj = nextJ[g];
-          const long long k = g + (long long)jj * C;
-          if (k >= nMine) continue;
-          const int buf = jj & 1;
-          if (!mbar_try_wait(&empty[2 * g + buf], (uint32_t)((jj >> 1) & 1) ^ 1u)) continue;
-          issue(k, g, buf);
-          nextJ[g] = jj + 1;
-          --remaining;
-          progress = true;
-        }
-        if (progress) {
-          idle0 = clock64();
-        } else {
-          if (clock64() - idle0 > a.waitCycles) {
-            abort = true;
-            break;
-          }
-          __nanosleep(32);
-        }
-      }
-      if (abort) {
-        if (a.err) atomicExch(a.err, 1);
-        // Wait (bounded) for the copies already issued into buffers no consumer
-        // will read any more, so none is in flight when the CTA exits.
-        for (int g = 0; g < C; ++g) {
-          for (int jj = (nextJ[g] > 2 ? nextJ[g] - 2 : 0); jj < nextJ[g]; ++jj)
-            mbar_wait(&full[2 * g + (jj & 1)], (uint32_t)((jj >> 1) & 1), a.waitCycles);
-        }
-      }
+  // Group g consumes the CTA's elements g, g + C, g + 2C, ... through its two
+  // buffers; its thread 0 issues the copies of local element jj + 2 into the
+  // buffer that element jj has just released.
+  const uint32_t qb = NV * PP * 8, gb = geo_record_doubles<P>() * 8, ob = 4 * TS * sizeof(R);
+  uint32_t xb[5] = {0, 0, 0, 0, 0};
+  if constexpr (kLSW) {
+    xb[0] = PP * 8;
+    xb[1] = 4 * P * 8;
+    xb[2] = a.fld[2] ? PP * 8 : 0;
+  } else if constexpr (kSW) {
+    xb[0] = a.fld[0] ? 4 * P * 8 : 0;
+    xb[1] = a.fld[1] ? 2 * PP * 8 : 0;
+  } else {
+    xb[0] = a.fld[0] ? 2 * PP * 8 : 0;
+    xb[1] = a.fld[1] ? PP * 8 : 0;
+    xb[2] = xb[3] = xb[4] = a.fld[2] ? 16 * P * 8 : 0;
+  }
+  auto issue = [&](long long jj) {  // thread 0 only
+    const long long k = g + jj * C;
+    if (k >= nMine) return;
+    const int buf = (int)(jj & 1);
+    const long long e = blockIdx.x + k * gridDim.x;
+    unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
+    uint64_t* bar = &full[2 * g + buf];
+    uint32_t bytes = qb + gb + ob + xb[0] + xb[1] + xb[2] + xb[3] + xb[4];
+    if constexpr (kSW) bytes += 8 * P * sizeof(R);
+    mbar_arrive_expect_tx(bar, bytes);
+    if (a.debugStarve && blockIdx.x == 0 && k == 0) return;
+    const R* trIn = reinterpret_cast<const R*>(a.trIn);
+    bulk_g2s(sl + pl.oQ, a.q + (size_t)e * NV * PP, qb, bar);
+    bulk_g2s(sl + pl.oDsdx, a.geo + (size_t)e * geo_record_doubles<P>(), gb, bar);
+    bulk_g2s(sl + pl.oOwn, trIn + (size_t)4 * TS * e, ob, bar);
+    if constexpr (kSW)
+      bulk_g2s(sl + pl.oVelOwn, reinterpret_cast<const R*>(a.velIn) + (size_t)e * 8 * P, 8 * P * sizeof(R), bar);
+    if constexpr (kLSW) {
+      bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * PP, xb[0], bar);
+      bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 4 * P, xb[1], bar);
+      if (xb[2]) bulk_g2s(sl + pl.oX[2], a.fld[2] + (size_t)e * PP, xb[2], bar);
+    } else if constexpr (kSW) {
+      if (xb[0]) bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * 4 * P, xb[0], bar);
+      if (xb[1]) bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 2 * PP, xb[1], bar);
+    } else {
+      if (xb[0]) bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * 4 * PP, xb[0], bar);
+      if (xb[1]) bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 2 * PP + PP, xb[1], bar);
+      if (xb[2])
+        for (int x = 2; x < 5; ++x) bulk_g2s(sl + pl.oX[x], a.fld[x] + (size_t)e * 16 * P, xb[x], bar);
     }
-    return;
+  };
+  if (t == 0) {
+    issue(0);
+    issue(1);
   }
 
-  // -------------------------------------------------------------- consumers
-  const int g = (threadIdx.x - 32) / TPE;
-  const int t = (threadIdx.x - 32) % TPE;
-  if (g >= C) return;
   const int barId = 1 + g;
   const bool active = t < PP;
   const int i = t % P, j = t / P;
@@ -282,7 +242,12 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     if (t == 0) gflag[g] = mbar_wait(&full[2 * g + buf], par, a.waitCycles) ? 1 : 0;
     named_bar(barId, TPE);
     if (!gflag[g]) {
-      if (t == 0 && a.err) atomicExch(a.err, 1);
+      if (t == 0) {
+        if (a.err) atomicExch(a.err, 1);
+        // Wait (bounded) for the group's other copy in flight, so that none is
+        // pending when the CTA exits.
+        if (k + C < nMine) mbar_wait(&full[2 * g + (buf ^ 1)], (uint32_t)(((jj + 1) >> 1) & 1), a.waitCycles);
+      }
       break;
     }
     const int* ssi = reinterpret_cast<const int*>(sl + pl.oSi);
@@ -502,7 +467,10 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       }
     }
     named_bar(barId, TPE);  // every thread is done reading the flux array and the buffer
-    if (t == 0) mbar_arrive(&empty[2 * g + buf]);
+    if (t == 0) {  // refill the buffer: generic-proxy reads before the async-proxy writes
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(jj + 2);
+    }
     if (!rk) {
       if (active)
 #pragma unroll
@@ -600,12 +568,12 @@ inline bool make_tma_plan(const StageArgs& a, int smemLimit, TmaPlan& pl, int ma
   const int cMax = (maxGroups > 0 && maxGroups < T::kMaxGroups) ? maxGroups : T::kMaxGroups;
   for (int C = cMax; C >= 1; --C) {
     int s = 0;
-    s += 4 * C * 8;  // barriers
+    s += 2 * C * 8;  // barriers
     s = (s + 15) / 16 * 16;
     const int oMats = s;
     s += (PP + 3 * P) * 8;
     const int oFlags = s;
-    s += 2 * C * 4;  // consumer flags, producer counters
+    s += C * 4;  // group flags
     s = (s + 127) / 128 * 128;
     const int oSlots = s;
     s += 2 * C * pl.slotBytes;

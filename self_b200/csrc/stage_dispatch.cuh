@@ -41,7 +41,7 @@ cudaError_t launch_one(const StageArgs& a, const StageLaunch& L, cudaStream_t st
       }
       using T = TmaTraits<P, Phys, R>;
       const int grid = a.nEl < L.numSMs ? a.nEl : L.numSMs;
-      k_fused_stage_tma<P, Phys, R><<<grid, 32 + pl.groups * T::TPE, pl.smemBytes, st>>>(a, pl);
+      k_fused_stage_tma<P, Phys, R><<<grid, pl.groups * T::TPE, pl.smemBytes, st>>>(a, pl);
       *usedTma = 1;
       return cudaGetLastError();
     }
