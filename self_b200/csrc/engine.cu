@@ -596,13 +596,13 @@ int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, f
   const StageLaunch saved = m->cfg;
   float best = 1e30f;
   StageLaunch bestCfg = saved;
-  for (int cand = 0; cand <= 8; ++cand) {
+  for (int cand = 0; cand <= 9; ++cand) {
     StageLaunch c = saved;
     if (cand == 0) {
       c.allowTma = false;
     } else {
       c.allowTma = true;
-      c.maxGroups = cand + 1;  // 2..9 consumer groups, capped by what fits
+      c.maxGroups = cand + 1;  // 2..10 consumer groups, capped by what fits
     }
     m->cfg = c;
     int tma = 0;

@@ -80,7 +80,7 @@ struct StageArgs {
   // bounded waits of the persistent kernel (clock cycles) and its error word
   long long waitCycles;
   int* err;
-  int debugStarve;  // test hook: the producer registers the first tile but issues no copies
+  int debugStarve;  // test hook: the first element of CTA 0 is registered on its mbarrier but never copied
   // operator matrices (Lagrange%Init): dgM(ii,i) at [ii + P*i], bM(ii,side), qw;
   // bMf holds bM rounded to float for the FP32-bulk form
   double dgM[kMaxP * kMaxP];
