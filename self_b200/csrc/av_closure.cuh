@@ -164,13 +164,13 @@ struct NuWarpSmem {
 // Orthonormal modal energies of one P x P field of this warp's element:
 // c(k,l) = sum_j T(l,j) sum_i T(k,i) q(i,j), then c^2 in place.
 template <int P, typename R>
-__device__ __forceinline__ void warp_modal_energy(const double* sT, const R* q, R* tt, R* c, int lane) {
+__device__ __forceinline__ void warp_modal_energy(const R* sT, const R* q, R* tt, R* c, int lane) {
   constexpr int PP = P * P;
   for (int o = lane; o < PP; o += 32) {
     const int k = o % P, jj = o / P;
     R acc = (R)0;
 #pragma unroll
-    for (int m = 0; m < P; ++m) acc = acc + (R)sT[k + P * m] * q[m + P * jj];
+    for (int m = 0; m < P; ++m) acc = acc + sT[k + P * m] * q[m + P * jj];
     tt[k + P * jj] = acc;
   }
   __syncwarp();
@@ -178,7 +178,7 @@ __device__ __forceinline__ void warp_modal_energy(const double* sT, const R* q, 
     const int k = o % P, l = o / P;
     R acc = (R)0;
 #pragma unroll
-    for (int m = 0; m < P; ++m) acc = acc + (R)sT[l + P * m] * tt[k + P * m];
+    for (int m = 0; m < P; ++m) acc = acc + sT[l + P * m] * tt[k + P * m];
     c[k + P * l] = acc * acc;
   }
   __syncwarp();
@@ -190,10 +190,10 @@ template <int P, typename R>
 __global__ void __launch_bounds__(32 * kNuWarps) k_av_nu(const AvArgs a) {
   constexpr int PP = P * P, N = P - 1;
   __shared__ NuWarpSmem<P, R> ws[kNuWarps];
-  __shared__ double sT[PP];
+  __shared__ R sT[PP];
   __shared__ float sW1[kMlpHidden * kMlpIn], sW2[kMlpHidden * kMlpHidden], sw3[kMlpHidden], sB[kMlpFloats];
   const bool mlp = (a.mode == AV_MLP) && (P >= 6);
-  for (int k = threadIdx.x; k < PP; k += blockDim.x) sT[k] = a.T[k];
+  for (int k = threadIdx.x; k < PP; k += blockDim.x) sT[k] = (R)a.T[k];
   if (mlp) {
     for (int k = threadIdx.x; k < kMlpHidden * kMlpIn; k += blockDim.x) sW1[k] = __bfloat162float(a.mlpW[k]);
     for (int k = threadIdx.x; k < kMlpHidden * kMlpHidden; k += blockDim.x)
@@ -206,8 +206,24 @@ __global__ void __launch_bounds__(32 * kNuWarps) k_av_nu(const AvArgs a) {
   const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
   NuWarpSmem<P, R>& s = ws[w];
   const R gam = (R)a.gamma;
-  for (long long e = (long long)blockIdx.x * kNuWarps + w; e < a.nEl; e += (long long)gridDim.x * kNuWarps) {
-    for (int k = lane; k < PP; k += 32) s.q[0][k] = (R)a.q[k + (long long)PP * (2 + 4 * e)];
+  // the density of the warp's next element is loaded into registers while
+  // the current one is processed (the loads' latency is the main cost)
+  constexpr int QPL = (PP + 31) / 32;  // density values per lane
+  const long long eStride = (long long)gridDim.x * kNuWarps;
+  double qn[QPL];
+  auto load_density = [&](long long e) {
+#pragma unroll
+    for (int r = 0; r < QPL; ++r) {
+      const int k = lane + 32 * r;
+      qn[r] = (e < a.nEl && k < PP) ? a.q[k + (long long)PP * (2 + 4 * e)] : 0.0;
+    }
+  };
+  load_density((long long)blockIdx.x * kNuWarps + w);
+  for (long long e = (long long)blockIdx.x * kNuWarps + w; e < a.nEl; e += eStride) {
+#pragma unroll
+    for (int r = 0; r < QPL; ++r)
+      if (lane + 32 * r < PP) s.q[0][lane + 32 * r] = (R)qn[r];
+    load_density(e + eStride);
     __syncwarp();
     warp_modal_energy<P, R>(sT, s.q[0], s.tt, s.c[0], lane);
     // fixed-order sums per eta-degree l, then over l
