@@ -36,9 +36,6 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -244,8 +241,9 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     if (!gflag[g]) {
       if (t == 0) {
         if (a.err) atomicExch(a.err, 1);
-        // Wait (bounded) for the group's other copy in flight, so that none is
-        // pending when the CTA exits.
+        // Wait (bounded) once more for this buffer's copies and for those of
+        // the group's other buffer, so that none is pending when the CTA exits.
+        mbar_wait(&full[2 * g + buf], par, a.waitCycles);
         if (k + C < nMine) mbar_wait(&full[2 * g + (buf ^ 1)], (uint32_t)(((jj + 1) >> 1) & 1), a.waitCycles);
       }
       break;
