@@ -156,6 +156,13 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) sb[k] = a.bM[k];
   for (int k = threadIdx.x; k < P; k += blockDim.x) sqw[k] = a.qw[k];
   __syncthreads();
+  // Launched as a programmatic dependent of the previous kernel on the stream:
+  // let the next launch start its own prologue, then wait until the previous
+  // kernel has completed and its writes are visible.  Everything above reads
+  // only set-up constants; everything below may read what it wrote or write
+  // what it read.  (Both are no-ops for an ordinary launch.)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
 
   const long long nMine =
       (long long)blockIdx.x < a.nEl ? ((long long)a.nEl - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;

@@ -41,9 +41,22 @@ cudaError_t launch_one(const StageArgs& a, const StageLaunch& L, cudaStream_t st
       }
       using T = TmaTraits<P, Phys, R>;
       const int grid = a.nEl < L.numSMs ? a.nEl : L.numSMs;
-      k_fused_stage_tma<P, Phys, R><<<grid, pl.groups * T::TPE, pl.smemBytes, st>>>(a, pl);
+      // Programmatic dependent launch: the launch and the kernel's prologue
+      // overlap the end of the previous kernel on the stream; the kernel waits
+      // for that kernel's completion (griddepcontrol.wait) before it touches
+      // any data the previous kernel may write or read.
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(grid);
+      cfg.blockDim = dim3(pl.groups * T::TPE);
+      cfg.dynamicSmemBytes = pl.smemBytes;
+      cfg.stream = st;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr[0].val.programmaticStreamSerializationAllowed = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
       *usedTma = 1;
-      return cudaGetLastError();
+      return cudaLaunchKernelEx(&cfg, k_fused_stage_tma<P, Phys, R>, a, pl);
     }
   }
   constexpr int EPB = elems_per_block<P, Phys, R>();
