@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 #include "fused_stage.cuh"
@@ -32,12 +33,17 @@ cudaError_t launch_one(const StageArgs& a, const StageLaunch& L, cudaStream_t st
     for (int k = 0; k < 5; ++k) ok = ok && (a.fld[k] == nullptr || aligned16(a.fld[k]));
     TmaPlan pl{};
     if (ok && make_tma_plan<P, Phys, R>(a, L.smemOptin, pl, L.maxGroups)) {
-      static bool attrSet = false;  // one instantiation per (P, Phys, R)
-      if (!attrSet) {
-        cudaError_t e = cudaFuncSetAttribute(k_fused_stage_tma<P, Phys, R>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, L.smemOptin);
+      // the shared-memory opt-in is per device: one bit per device that has it
+      static std::atomic<unsigned long long> attrSet{0};  // one instantiation per (P, Phys, R)
+      int dev = 0;
+      cudaError_t e = cudaGetDevice(&dev);
+      if (e != cudaSuccess) return e;
+      const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+      if (!(attrSet.load() & bit)) {
+        e = cudaFuncSetAttribute(k_fused_stage_tma<P, Phys, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 L.smemOptin);
         if (e != cudaSuccess) return e;
-        attrSet = true;
+        attrSet.fetch_or(bit);
       }
       using T = TmaTraits<P, Phys, R>;
       const int grid = a.nEl < L.numSMs ? a.nEl : L.numSMs;
