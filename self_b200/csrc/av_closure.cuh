@@ -36,6 +36,8 @@
 
 #include <cuda_bf16.h>
 
+#include <atomic>
+
 #include "fused_stage.cuh"
 
 namespace selfgpu {
@@ -545,8 +547,18 @@ template <int P, typename R>
 cudaError_t launch_av_pair(const AvArgs& a, cudaStream_t st, int numSMs) {
   cudaError_t e = cudaMemsetAsync(a.activeCount, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
+  // one wave of resident blocks, each warp striding over its share of the
+  // elements (a partial second wave would run at low occupancy)
+  static std::atomic<int> nuPerSM{0};  // resident blocks per SM, one instantiation per (P, R)
+  if (nuPerSM.load() == 0) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_av_nu<P, R>, 32 * kNuWarps, 0) != cudaSuccess || nb < 1)
+      nb = 4;
+    nuPerSM.store(nb);
+  }
   const long long nuBlocks = (a.nEl + kNuWarps - 1) / kNuWarps;
-  const int g1 = (int)(nuBlocks < 16LL * numSMs ? nuBlocks : 16LL * numSMs);
+  const long long cap = (long long)nuPerSM.load() * numSMs;
+  const int g1 = (int)(nuBlocks < cap ? nuBlocks : cap);
   k_av_nu<P, R><<<g1, 32 * kNuWarps, 0, st>>>(a);
   constexpr int EPB = av_elems_per_block<P, R>();
   k_av_grad<P, R, EPB><<<4 * numSMs, EPB * P * P, 0, st>>>(a);
