@@ -8,9 +8,11 @@
 // viscosity per element instead of one diffusivity.
 //
 // With the closure on, each RK stage runs, before the stage kernel:
-//   k_av_nu     one warp per element: the element viscosity nu (modal-decay
-//               indicator of the density, or the closure MLP with the indicator
-//               as fallback and screen), and the list of elements with nu > 0;
+//   k_av_nu     the element viscosity nu (modal-decay indicator of the
+//               density, or the closure MLP with the indicator as fallback and
+//               screen), and the list of elements with nu > 0: in FP32 one lane
+//               per element for the indicator, warp-wide for the few elements
+//               that need the MLP or the wave speed; in FP64 one warp per element;
 //   k_av_grad   the listed elements only: the BR1 gradient of the four
 //               conservative variables from the averaged traces of the stage's
 //               trace cache, the contravariant viscous volume flux
@@ -159,6 +161,7 @@ struct NuWarpSmem {
   R tt[PP];
   R c[2][PP];  // modal energies c^2
   R part[3][P];
+  R act[32], lam[32];  // per lane's element (FP32 lane-per-element path)
   float feat[kMlpIn];
   float h1[kMlpHidden];
 };
@@ -188,6 +191,137 @@ __device__ __forceinline__ void warp_modal_energy(const R* sT, const R* q, R* tt
 
 constexpr int kNuWarps = 4;
 
+// The closure MLP's activation for element e (warp-wide): the density and
+// total-energy modes, the 36 features, the two hidden layers and the clamped
+// output; the indicator activation actInd stays when a feature lies outside
+// the training range (counted).  Lane 0's result is returned on every lane.
+template <int P, typename R>
+__device__ R warp_mlp_act(const AvArgs& a, const R* sT, NuWarpSmem<P, R>& s, const float* sW1, const float* sW2,
+                          const float* sw3, const float* sB, long long e, int lane, R actInd) {
+  constexpr int PP = P * P, N = P - 1;
+  R act = actInd;
+  for (int k = lane; k < PP; k += 32) {
+    s.q[0][k] = (R)a.q[k + (long long)PP * (2 + 4 * e)];
+    s.q[1][k] = (R)a.q[k + (long long)PP * (3 + 4 * e)];
+  }
+  __syncwarp();
+  warp_modal_energy<P, R>(sT, s.q[0], s.tt, s.c[0], lane);
+  warp_modal_energy<P, R>(sT, s.q[1], s.tt, s.c[1], lane);
+  if (lane < P) {  // fixed-order sums per eta-degree l, then over l
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      R tot = (R)0;
+#pragma unroll
+      for (int k = 0; k < P; ++k) tot = tot + s.c[r][k + P * lane];
+      s.part[r][lane] = tot;
+    }
+  }
+  __syncwarp();
+  if (lane < 2) {
+    R total = (R)0;
+#pragma unroll
+    for (int l = 0; l < P; ++l) total = total + s.part[lane][l];
+    s.part[2][lane] = total;
+  }
+  __syncwarp();
+  for (int f = lane; f < kMlpIn; f += 32) {
+    const int r = f / 18, grp = (f % 18) / 6, m = N - 5 + f % 6;
+    const R* e2 = s.c[r];
+    R sum = (R)0;
+    if (grp == 0) {
+      for (int l = 0; l < m; ++l) sum = sum + e2[m + P * l];
+      for (int k = 0; k <= m; ++k) sum = sum + e2[k + P * m];
+    } else if (grp == 1) {
+      for (int l = 0; l < P; ++l) sum = sum + e2[m + P * l];
+    } else {
+      for (int k = 0; k < P; ++k) sum = sum + e2[k + P * m];
+    }
+    const R total = s.part[2][r];
+    R qf = total > (R)0 ? sum / total : (R)0;
+    if (qf < (R)1e-16) qf = (R)1e-16;
+    s.feat[f] = (float)((av_log10<R>(qf) + (R)8) / (R)8);
+  }
+  __syncwarp();
+  {
+    float acc = 0.f;  // lane = hidden unit
+#pragma unroll 4
+    for (int k = 0; k < kMlpIn; ++k) acc = fmaf(sW1[lane * kMlpIn + k], s.feat[k], acc);
+    acc = acc + sB[lane];
+    s.h1[lane] = acc > 0.f ? acc : 0.f;
+  }
+  __syncwarp();
+  float h2;
+  {
+    float acc = 0.f;
+#pragma unroll 4
+    for (int k = 0; k < kMlpHidden; ++k) acc = fmaf(sW2[lane * kMlpHidden + k], s.h1[k], acc);
+    acc = acc + sB[kMlpHidden + lane];
+    h2 = acc > 0.f ? acc : 0.f;
+  }
+  __syncwarp();
+  s.h1[lane] = h2;  // the second hidden layer reuses the first's array
+  __syncwarp();
+  if (lane == 0) {
+    if (a.fallbacks) atomicAdd(a.fallbacks + 1, 1);
+    bool inRange = true;
+    const float* fmin = sB + 2 * kMlpHidden + 1;
+    const float* fmax = fmin + kMlpIn;
+    for (int k = 0; k < kMlpIn; ++k)
+      inRange = inRange && s.feat[k] >= fmin[k] - kMlpRangeMargin && s.feat[k] <= fmax[k] + kMlpRangeMargin;
+    if (inRange) {
+      float z = 0.f;
+      for (int k = 0; k < kMlpHidden; ++k) z = fmaf(sw3[k], s.h1[k], z);
+      z = z + sB[2 * kMlpHidden];
+      act = (R)(z < 0.f ? 0.f : (z > 1.f ? 1.f : z));
+    } else if (a.fallbacks) {
+      atomicAdd(a.fallbacks, 1);
+    }
+  }
+  act = __shfl_sync(0xffffffffu, act, 0);
+  __syncwarp();
+  return act;
+}
+
+// Wave speed |u| + c of element e, max over its nodes (warp-wide;
+// src/models/SELF_CompressibleIdealGas2D.f90:1090-1110).
+template <int P, typename R>
+__device__ R warp_wave_speed(const AvArgs& a, long long e, int lane) {
+  constexpr int PP = P * P;
+  const R gam = (R)a.gamma;
+  R lam = (R)0;
+  for (int k = lane; k < PP; k += 32) {
+    const long long b = k + (long long)PP * 4 * e;
+    const R ru = (R)a.q[b], rv = (R)a.q[b + PP], rho = (R)a.q[b + 2 * PP], rE = (R)a.q[b + 3 * PP];
+    const R u = ru / rho, v = rv / rho;
+    const R ke = (R)0.5 * (ru * u + rv * v);
+    const R p = (gam - (R)1) * (rE - ke);
+    const R c = av_sqrt<R>(gam * p / rho);
+    const R wv = av_sqrt<R>(u * u + v * v) + c;
+    if (wv > lam) lam = wv;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const R other = __shfl_xor_sync(0xffffffffu, lam, o);
+    if (other > lam) lam = other;
+  }
+  return lam;
+}
+
+// Indicator activation from the totals of all modal energies and of the top
+// shell, and whether the MLP must be evaluated (not screened out).
+template <typename R>
+__device__ __forceinline__ void indicator_act(const AvArgs& a, R total, R top, bool mlp, R& actInd, int& need) {
+  actInd = (R)0;
+  need = 0;
+  if (top > (R)0 && total > (R)0) {
+    const R sv = av_log10<R>(top / total);
+    if (sv > (R)a.s0 + (R)a.kappa) actInd = (R)1;
+    else if (!(sv < (R)a.s0 - (R)a.kappa))
+      actInd = (R)0.5 * ((R)1 + av_sin<R>((R)kAvPi * (sv - (R)a.s0) / ((R)2 * (R)a.kappa)));
+    need = mlp && !(sv < (R)(a.s0 - a.kappa - kMlpGate));
+  }
+}
+
 template <int P, typename R>
 __global__ void __launch_bounds__(32 * kNuWarps) k_av_nu(const AvArgs a) {
   constexpr int PP = P * P, N = P - 1;
@@ -207,6 +341,96 @@ __global__ void __launch_bounds__(32 * kNuWarps) k_av_nu(const AvArgs a) {
   __syncthreads();
   const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
   NuWarpSmem<P, R>& s = ws[w];
+  if constexpr (sizeof(R) == 4) {
+    // FP32: one lane per element for the indicator (the warp's 32 elements
+    // are spread over the mesh, so that the few that need the MLP or the wave
+    // speed, done warp-wide, are spread over the warps too)
+    const long long nW = (long long)gridDim.x * kNuWarps;
+    for (long long base = (long long)blockIdx.x * kNuWarps + w; base < a.nEl; base += 32 * nW) {
+      const long long e = base + (long long)lane * nW;
+      R actInd = (R)0;
+      int need = 0;
+      if (e < a.nEl) {
+        // density modes: the operations and summation orders of warp_modal_energy
+        // and of the per-eta-degree sums
+        R q[PP];
+        const double2* qg = reinterpret_cast<const double2*>(a.q + (long long)PP * (2 + 4 * e));
+#pragma unroll
+        for (int k = 0; k < PP / 2; ++k) {
+          const double2 x = qg[k];
+          q[2 * k] = (R)x.x;
+          q[2 * k + 1] = (R)x.y;
+        }
+        if constexpr (PP % 2) q[PP - 1] = (R)a.q[(long long)PP * (2 + 4 * e) + PP - 1];
+        R tot[P], top[P];
+#pragma unroll
+        for (int l = 0; l < P; ++l) tot[l] = top[l] = (R)0;
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+          R tt[P];
+#pragma unroll
+          for (int jj = 0; jj < P; ++jj) {
+            R acc = (R)0;
+#pragma unroll
+            for (int m = 0; m < P; ++m) acc = acc + sT[k + P * m] * q[m + P * jj];
+            tt[jj] = acc;
+          }
+#pragma unroll
+          for (int l = 0; l < P; ++l) {
+            R acc = (R)0;
+#pragma unroll
+            for (int m = 0; m < P; ++m) acc = acc + sT[l + P * m] * tt[m];
+            const R c = acc * acc;
+            tot[l] = tot[l] + c;
+            if (k == N) top[l] = c;
+          }
+        }
+        top[N] = tot[N];
+        R total = (R)0, topS = (R)0;
+#pragma unroll
+        for (int l = 0; l < P; ++l) {
+          total = total + tot[l];
+          topS = topS + top[l];
+        }
+        indicator_act<R>(a, total, topS, mlp, actInd, need);
+      }
+      s.act[lane] = actInd;
+      const unsigned needMask = __ballot_sync(0xffffffffu, need);
+      __syncwarp();
+      for (unsigned mk = needMask; mk; mk &= mk - 1) {
+        const int b = __ffs(mk) - 1;
+        const R act = warp_mlp_act<P, R>(a, sT, s, sW1, sW2, sw3, sB, base + (long long)b * nW, lane,
+                                         __shfl_sync(0xffffffffu, actInd, b));
+        if (lane == 0) s.act[b] = act;
+        __syncwarp();
+      }
+      const R act = s.act[lane];
+      const unsigned actMask = __ballot_sync(0xffffffffu, e < a.nEl && act != (R)0);
+      for (unsigned mk = actMask; mk; mk &= mk - 1) {
+        const int b = __ffs(mk) - 1;
+        const R lam = warp_wave_speed<P, R>(a, base + (long long)b * nW, lane);
+        if (lane == 0) s.lam[b] = lam;
+      }
+      __syncwarp();
+      double nu = 0.0;
+      if (e < a.nEl) {
+        if (act != (R)0) nu = (double)act * a.avC * a.hEl[e] / (double)N * (double)s.lam[lane];
+        a.nu[e] = nu;
+        a.act[e] = (float)act;
+        if (mlp && a.actInd) a.actInd[e] = (float)actInd;
+      }
+      const unsigned nzMask = __ballot_sync(0xffffffffu, nu != 0.0);
+      if (nzMask) {
+        int b0 = 0;
+        if (lane == 0) b0 = atomicAdd(a.activeCount, __popc(nzMask));
+        b0 = __shfl_sync(0xffffffffu, b0, 0);
+        if (nu != 0.0) a.activeList[b0 + __popc(nzMask & ((1u << lane) - 1u))] = (int)e;
+      }
+      __syncwarp();
+    }
+    return;
+  }
+  // FP64: one warp per element
   const R gam = (R)a.gamma;
   // the density of the warp's next element is loaded into registers while
   // the current one is processed (the loads' latency is the main cost)
