@@ -431,7 +431,6 @@ __global__ void __launch_bounds__(32 * kNuWarps) k_av_nu(const AvArgs a) {
     return;
   }
   // FP64: one warp per element
-  const R gam = (R)a.gamma;
   // the density of the warp's next element is loaded into registers while
   // the current one is processed (the loads' latency is the main cost)
   constexpr int QPL = (PP + 31) / 32;  // density values per lane
@@ -471,113 +470,14 @@ __global__ void __launch_bounds__(32 * kNuWarps) k_av_nu(const AvArgs a) {
         total = total + s.part[0][l];
         top = top + s.part[1][l];
       }
-      if (top > (R)0 && total > (R)0) {
-        const R sv = av_log10<R>(top / total);
-        if (sv > (R)a.s0 + (R)a.kappa) actInd = (R)1;
-        else if (!(sv < (R)a.s0 - (R)a.kappa))
-          actInd = (R)0.5 * ((R)1 + av_sin<R>((R)kAvPi * (sv - (R)a.s0) / ((R)2 * (R)a.kappa)));
-        need = mlp && !(sv < (R)(a.s0 - a.kappa - kMlpGate));
-      }
-      s.part[2][0] = total;
+      indicator_act<R>(a, total, top, mlp, actInd, need);
     }
     actInd = __shfl_sync(0xffffffffu, actInd, 0);
     need = __shfl_sync(0xffffffffu, need, 0);
-    R act = actInd;
-    if (need) {
-      // the closure MLP: features of the density and total-energy modes
-      for (int k = lane; k < PP; k += 32) s.q[1][k] = (R)a.q[k + (long long)PP * (3 + 4 * e)];
-      __syncwarp();
-      warp_modal_energy<P, R>(sT, s.q[1], s.tt, s.c[1], lane);
-      if (lane < P) {
-        R tot = (R)0;
-#pragma unroll
-        for (int k = 0; k < P; ++k) tot = tot + s.c[1][k + P * lane];
-        s.part[1][lane] = tot;
-      }
-      __syncwarp();
-      if (lane == 0) {
-        R total = (R)0;
-#pragma unroll
-        for (int l = 0; l < P; ++l) total = total + s.part[1][l];
-        s.part[2][1] = total;
-      }
-      __syncwarp();
-      for (int f = lane; f < kMlpIn; f += 32) {
-        const int r = f / 18, grp = (f % 18) / 6, m = N - 5 + f % 6;
-        const R* e2 = s.c[r];
-        R sum = (R)0;
-        if (grp == 0) {
-          for (int l = 0; l < m; ++l) sum = sum + e2[m + P * l];
-          for (int k = 0; k <= m; ++k) sum = sum + e2[k + P * m];
-        } else if (grp == 1) {
-          for (int l = 0; l < P; ++l) sum = sum + e2[m + P * l];
-        } else {
-          for (int k = 0; k < P; ++k) sum = sum + e2[k + P * m];
-        }
-        const R total = s.part[2][r];
-        R qf = total > (R)0 ? sum / total : (R)0;
-        if (qf < (R)1e-16) qf = (R)1e-16;
-        s.feat[f] = (float)((av_log10<R>(qf) + (R)8) / (R)8);
-      }
-      __syncwarp();
-      {
-        float acc = 0.f;  // lane = hidden unit
-#pragma unroll 4
-        for (int k = 0; k < kMlpIn; ++k) acc = fmaf(sW1[lane * kMlpIn + k], s.feat[k], acc);
-        acc = acc + sB[lane];
-        s.h1[lane] = acc > 0.f ? acc : 0.f;
-      }
-      __syncwarp();
-      float h2;
-      {
-        float acc = 0.f;
-#pragma unroll 4
-        for (int k = 0; k < kMlpHidden; ++k) acc = fmaf(sW2[lane * kMlpHidden + k], s.h1[k], acc);
-        acc = acc + sB[kMlpHidden + lane];
-        h2 = acc > 0.f ? acc : 0.f;
-      }
-      __syncwarp();
-      s.h1[lane] = h2;  // the second hidden layer reuses the first's array
-      __syncwarp();
-      if (lane == 0) {
-        if (a.fallbacks) atomicAdd(a.fallbacks + 1, 1);
-        bool inRange = true;
-        const float* fmin = sB + 2 * kMlpHidden + 1;
-        const float* fmax = fmin + kMlpIn;
-        for (int k = 0; k < kMlpIn; ++k)
-          inRange = inRange && s.feat[k] >= fmin[k] - kMlpRangeMargin && s.feat[k] <= fmax[k] + kMlpRangeMargin;
-        if (inRange) {
-          float z = 0.f;
-          for (int k = 0; k < kMlpHidden; ++k) z = fmaf(sw3[k], s.h1[k], z);
-          z = z + sB[2 * kMlpHidden];
-          act = (R)(z < 0.f ? 0.f : (z > 1.f ? 1.f : z));
-        } else if (a.fallbacks) {
-          atomicAdd(a.fallbacks, 1);
-        }
-      }
-      act = __shfl_sync(0xffffffffu, act, 0);
-    }
+    __syncwarp();
+    const R act = need ? warp_mlp_act<P, R>(a, sT, s, sW1, sW2, sw3, sB, e, lane, actInd) : actInd;
     double nu = 0.0;
-    if (act != (R)0) {
-      // wave speed |u| + c (src/models/SELF_CompressibleIdealGas2D.f90:1090-1110), max over the nodes
-      R lam = (R)0;
-      for (int k = lane; k < PP; k += 32) {
-        const long long b = k + (long long)PP * 4 * e;
-        const R ru = (R)a.q[b], rv = (R)a.q[b + PP], rho = (R)a.q[b + 2 * PP], rE = (R)a.q[b + 3 * PP];
-        const R u = ru / rho, v = rv / rho;
-        const R ke = (R)0.5 * (ru * u + rv * v);
-        const R p = (gam - (R)1) * (rE - ke);
-        const R c = av_sqrt<R>(gam * p / rho);
-        const R wv = av_sqrt<R>(u * u + v * v) + c;
-        if (wv > lam) lam = wv;
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const R other = __shfl_xor_sync(0xffffffffu, lam, o);
-        if (other > lam) lam = other;
-      }
-      nu = (double)act * a.avC * a.hEl[e] / (double)N * (double)lam;
-    }
+    if (act != (R)0) nu = (double)act * a.avC * a.hEl[e] / (double)N * (double)warp_wave_speed<P, R>(a, e, lane);
     if (lane == 0) {
       a.nu[e] = nu;
       a.act[e] = (float)act;
