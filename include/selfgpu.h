@@ -211,7 +211,9 @@ int selfgpu_lagrange_init(int N, int controlNodeType, int M, int targetNodeType,
  * nodeCoords(1:2,0:1,0:1,nEl), globalNodeIDs(0:1,0:1,nEl), sideInfo(1:5,1:4,nEl).
  * Periodic directions connect through bcid = 0; perturbation moves interior
  * nodes by perturbation*h*sin(2 pi x)sin(2 pi y); rotation (optional, nEl
- * entries) relabels an element's corners by quarter turns. */
+ * entries) relabels an element's corners by quarter turns.  A periodic
+ * direction may be one element wide (the element is then its own neighbour
+ * across it); rotated elements need two or more there (SELFGPU_ERR_ARG). */
 int selfgpu_mesh2d_structured(int nx, int ny, double x0, double x1, double y0, double y1, int periodicX,
                               int periodicY, double perturbation, int bcid, const int* rotation,
                               double* nodeCoords, int* globalNodeIDs, int* sideInfo);

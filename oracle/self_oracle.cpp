@@ -33,6 +33,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <tuple>
 #include <utility>
 #include <vector>
 #ifdef _OPENMP
@@ -845,15 +846,28 @@ struct Mesh2D {
           globalNodeIDs[i + 2 * (j + 2 * e)] = nodeId(gx, gy);
         }
       }
-    // Connectivity from shared corner pairs.
-    std::map<std::pair<int, int>, std::vector<std::pair<int, int>>> faces;
+    // Connectivity: sides on the same grid edge (orientation and lower-left
+    // grid node, wrapped where periodic) are neighbours; edges are numbered in
+    // the order of their corner-id pairs.  (Corner ids alone cannot separate
+    // the two edges of a periodic row one or two elements wide.)
+    std::map<std::tuple<int, int, int>, std::vector<std::pair<int, int>>> faces;
     auto corner = [&](int e, int c) {
       return globalNodeIDs[CGNSCorner[c][0] + 2 * (CGNSCorner[c][1] + 2 * e)];
+    };
+    auto edge = [&](int e, int s) {
+      int ix = e % nx, iy = e / nx;
+      int r = rot ? (((rot[e] % 4) + 4) % 4) : 0;
+      int ka = (CGNSSide[s][0] - 1 + r) % 4, kb = (CGNSSide[s][1] - 1 + r) % 4;
+      int xa = ix + off[ka][0], ya = iy + off[ka][1], xb = ix + off[kb][0], yb = iy + off[kb][1];
+      int gx = std::min(xa, xb), gy = std::min(ya, yb);
+      if (perX) gx %= nx;
+      if (perY) gy %= ny;
+      return 2 * (gx + (nx + 1) * gy) + (xa == xb ? 1 : 0);
     };
     for (int e = 0; e < nElem; ++e)
       for (int s = 0; s < 4; ++s) {
         int a = corner(e, CGNSSide[s][0] - 1), b = corner(e, CGNSSide[s][1] - 1);
-        faces[{std::min(a, b), std::max(a, b)}].push_back({e, s});
+        faces[{std::min(a, b), std::max(a, b), edge(e, s)}].push_back({e, s});
       }
     int gid = 0;
     for (auto& kv : faces) {

@@ -21,6 +21,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -237,8 +238,14 @@ const int kCornerIJ[4][2] = {{0, 0}, {1, 0}, {1, 1}, {0, 1}};
 int mesh2d_structured(int nx, int ny, double x0, double x1, double y0, double y1, int perX, int perY, double amp,
                       int bcid, const int* rot, double* nodeCoords, int* gnid, int* sideInfo) {
   if (nx < 1 || ny < 1) return set_error(SELFGPU_ERR_ARG, "mesh2d_structured: nx, ny must be >= 1");
-  if ((perX && nx < 2) || (perY && ny < 2))
-    return set_error(SELFGPU_ERR_ARG, "mesh2d_structured: a periodic direction needs >= 2 elements");
+  // With one element across a periodic direction, both corners of the edges
+  // along it are one node, and the flip of a rotated element's side could not
+  // be read from the corner ids.
+  if (rot && ((perX && nx == 1) || (perY && ny == 1)))
+    for (int e = 0; e < nx * ny; ++e)
+      if (((rot[e] % 4) + 4) % 4 != 0)
+        return set_error(SELFGPU_ERR_ARG,
+                         "mesh2d_structured: rotated elements need >= 2 elements across a periodic direction");
   const int nEl = nx * ny;
   const double hx = (x1 - x0) / nx, hy = (y1 - y0) / ny, h = std::min(hx, hy);
   const int rowLen = perX ? nx : nx + 1;
@@ -269,11 +276,28 @@ int mesh2d_structured(int nx, int ny, double x0, double x1, double y0, double y1
       }
     }
   auto corner_id = [&](int e, int c) { return gnid[kCornerIJ[c][0] + 2 * (kCornerIJ[c][1] + 2 * (size_t)e)]; };
-  std::map<std::pair<int, int>, std::vector<std::pair<int, int>>> faces;
+  // Sides are matched by the grid edge they lie on (orientation and lower-left
+  // grid node, wrapped in the periodic directions) and ordered by their corner
+  // ids.  The corner ids alone do not tell edges apart when a periodic
+  // direction is one or two elements wide (the two edges of such a row share
+  // both corner nodes).
+  auto edge_code = [&](int e, int s) {
+    const int ix = e % nx, iy = e / nx;
+    const int r = rot ? ((rot[e] % 4) + 4) % 4 : 0;
+    const int ca = (kSideCorners[s][0] + r) % 4, cb = (kSideCorners[s][1] + r) % 4;
+    const int xa = ix + kCornerIJ[ca][0], ya = iy + kCornerIJ[ca][1];
+    const int xb = ix + kCornerIJ[cb][0], yb = iy + kCornerIJ[cb][1];
+    const int vertical = (xa == xb);
+    int gx = std::min(xa, xb), gy = std::min(ya, yb);
+    if (perX) gx %= nx;
+    if (perY) gy %= ny;
+    return 2 * (gx + (nx + 1) * gy) + vertical;
+  };
+  std::map<std::tuple<int, int, int>, std::vector<std::pair<int, int>>> faces;
   for (int e = 0; e < nEl; ++e)
     for (int s = 0; s < 4; ++s) {
       int a = corner_id(e, kSideCorners[s][0]), b = corner_id(e, kSideCorners[s][1]);
-      faces[{std::min(a, b), std::max(a, b)}].push_back({e, s});
+      faces[{std::min(a, b), std::max(a, b), edge_code(e, s)}].push_back({e, s});
     }
   int gid = 0;
   for (auto& kv : faces) {

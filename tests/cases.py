@@ -23,6 +23,16 @@ def mesh_kwargs(kind):
                         rot=[0, 1, 2, 3, 2, 0, 3, 1, 1, 3, 0, 2]),
         "prescribed": dict(nx=3, ny=3, bcid=O.BC_PRESCRIBED, amp=0.03),
         "radiation": dict(nx=3, ny=3, bcid=O.BC_RADIATION, amp=0.0),
+        # edge cases: one element, one column, one row, the smallest periodic
+        # mesh (each element meets the other on both sides) with rotated
+        # elements, a column periodic across its one-element width (each
+        # element is its own east/west neighbour) and one fully periodic element
+        "single": dict(nx=1, ny=1, bcid=O.BC_NONORMALFLOW, amp=0.0),
+        "ring": dict(nx=1, ny=4, periodic=(True, False), bcid=O.BC_NONORMALFLOW, amp=0.0),
+        "torus": dict(nx=1, ny=1, periodic=(True, True), amp=0.0),
+        "column": dict(nx=1, ny=5, bcid=O.BC_NONORMALFLOW, amp=0.0),
+        "row": dict(nx=7, ny=1, bcid=O.BC_RADIATION, amp=0.0),
+        "pair": dict(nx=2, ny=2, periodic=(True, True), amp=0.05, rot=[3, 0, 2, 1]),
     }[kind]
 
 

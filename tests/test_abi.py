@@ -60,6 +60,54 @@ def test_mesh_generator_matches_oracle(kw):
     np.testing.assert_array_equal(m.nodeCoords, o.nodeCoords)
 
 
+def _grid_neighbour(nx, ny, periodic, e, s):
+    """Unrotated structured grid: the neighbour element and side across local
+    side s (0..3 = south, east, north, west) of element e, or None on a
+    physical boundary."""
+    ix, iy = e % nx, e // nx
+    dx, dy = ((0, -1), (1, 0), (0, 1), (-1, 0))[s]
+    jx, jy = ix + dx, iy + dy
+    if periodic[0]:
+        jx %= nx
+    if periodic[1]:
+        jy %= ny
+    if not (0 <= jx < nx and 0 <= jy < ny):
+        return None
+    return jx + nx * jy, (s + 2) % 4
+
+
+@pytest.mark.parametrize("nx,ny,periodic", [
+    (1, 1, (True, True)), (1, 4, (True, False)), (4, 1, (False, True)), (2, 1, (True, False)),
+    (2, 2, (True, True)), (2, 3, (True, True)), (1, 1, (False, False)), (3, 2, (False, True)),
+])
+def test_narrow_periodic_meshes_connect_grid_neighbours(nx, ny, periodic):
+    """Periodic directions one or two elements wide: the two edges of such a
+    row share both corner nodes, so sides are matched by their grid edge.
+    Every side must meet exactly its grid neighbour (itself across a
+    one-element periodic width) with flip 0, and the oracle agrees."""
+    m = S.Mesh2D(nx, ny, periodic=periodic, bcid=O.BC_NONORMALFLOW)
+    o = O.Mesh(nx, ny, periodic=periodic, bcid=O.BC_NONORMALFLOW)
+    np.testing.assert_array_equal(m.sideInfo, o.sideInfo)
+    for e in range(nx * ny):
+        for s in range(4):
+            si = m.sideInfo[:, s, e]
+            nb = _grid_neighbour(nx, ny, periodic, e, s)
+            if nb is None:
+                assert (si[2], si[3], si[4]) == (0, 0, O.BC_NONORMALFLOW), (e, s, si)
+            else:
+                assert (si[2] - 1, si[3] // 10 - 1, si[3] % 10, si[4]) == (nb[0], nb[1], 0, 0), (e, s, si)
+    # global side ids: each interior edge once as +id and once as -id
+    ids = m.sideInfo[1][m.sideInfo[4] == 0]
+    assert sorted(ids[ids > 0]) == sorted(-ids[ids < 0])
+
+
+def test_rotation_needs_two_elements_across_a_periodic_direction():
+    with pytest.raises(S.SelfGpuError, match="rotated elements"):
+        S.Mesh2D(1, 3, periodic=(True, False), rotation=[0, 1, 0])
+    S.Mesh2D(1, 3, periodic=(True, False), rotation=[0, 0, 0])
+    S.Mesh2D(2, 3, periodic=(True, False), rotation=[0, 1, 2, 3, 0, 1])
+
+
 def test_side_info_validation_rejects_malformed_records():
     m = S.Mesh2D(3, 3, periodic=(True, True))
     L = _lib.lib()
