@@ -222,6 +222,46 @@ def test_persistent_kernel_matches_per_element_kernel_bitwise(model, N):
     np.testing.assert_array_equal(outs[0], outs[1])
 
 
+@pytest.mark.parametrize("model,N", [("CIG", 7), ("SW", 5), ("LSW", 7)])
+def test_rk3_graph_steps_match_separate_stage_launches_bitwise(model, N):
+    """On a mesh with several elements per CTA, ForwardStep (graph-replayed
+    steps, each stage launched as a programmatic dependent of the previous
+    one) and the same stages issued one by one through selfgpu_model2d_stage
+    (the multi-rank entry point) give bit-identical states over two calls."""
+    import self_b200 as S
+    L = S.lib()
+    n, dt = 4, 2e-4
+    outs = []
+    for graphed in (True, False):
+        mesh = S.Mesh2D(24, 20, periodic=(True, True), perturbation=0.05)
+        geo = S.SEMQuad(S.Lagrange(N, S.GAUSS, N, S.UNIFORM), mesh)
+        cls = {"LSW": S.LinearShallowWater, "SW": S.ShallowWater, "CIG": S.CompressibleIdealGas2D}[model]
+        mod = cls(mesh, geo)
+        x = S.to_host(geo.x)
+        aux = C.aux_fields(model, x, 9)
+        if model == "LSW":
+            mod.SetBathymetry(aux["H"])
+            mod.SetCoriolis(aux["fCori"])
+        elif model == "SW":
+            mod.SetTopography(aux["topography"])
+        else:
+            mod.SetGravity(aux["gravityPotential"])
+            mod.SetDrag(aux["drag"])
+        mod.SetSolution(C.initial_state(model, x, 9))
+        if graphed:
+            mod.ForwardStep(n, dt)
+            mod.ForwardStep(n, dt)
+        else:
+            S.check(L.selfgpu_model2d_prologue(mod._h))
+            for _ in range(2 * n):
+                for st in range(3):
+                    S.check(L.selfgpu_model2d_stage(mod._h, dt, st))
+        mod.Sync()
+        outs.append(S.to_host(mod.solution).copy())
+    assert np.isfinite(outs[0]).all()
+    np.testing.assert_array_equal(outs[0], outs[1])
+
+
 def test_bounded_wait_timeout_is_reported_and_context_survives():
     """A stalled copy (registered, never issued) makes the consumers' bounded
     wait run out: the kernel returns, sync reports SELFGPU_ERR_TIMEOUT (6), and
