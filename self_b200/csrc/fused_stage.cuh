@@ -520,15 +520,25 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
       Phys::template source<double>(qd, na, a, Src);
       const double Jij = a.J[gnode];
       const R wi = (R)srw[i], wj = (R)srw[j];
+      // FP32 bulk: products with the reciprocals (the FP64 form divides as the reference does)
+      const R rwi = (R)(1.0 / srw[i]), rwj = (R)(1.0 / srw[j]);
+      const double rJ = 1.0 / Jij;
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
         R d = (R)0;
 #pragma unroll
         for (int m = 0; m < P; ++m)
           d = d + (R)sdg[m + P * i] * sm.Fc[0][v][m + P * j] + (R)sdg[m + P * j] * sm.Fc[1][v][i + P * m];
-        d = d + ((R)sb[i + P] * sm.fb[1][v][j] + (R)sb[i] * sm.fb[3][v][j]) / wi +
-            ((R)sb[j + P] * sm.fb[2][v][i] + (R)sb[j] * sm.fb[0][v][i]) / wj;
-        const double dsdt = Src[v] - (double)d / Jij;
+        const R lx = (R)sb[i + P] * sm.fb[1][v][j] + (R)sb[i] * sm.fb[3][v][j];
+        const R ly = (R)sb[j + P] * sm.fb[2][v][i] + (R)sb[j] * sm.fb[0][v][i];
+        double dsdt;
+        if constexpr (sizeof(R) == 8) {
+          d = d + lx / wi + ly / wj;
+          dsdt = Src[v] - (double)d / Jij;
+        } else {
+          d = d + lx * rwi + ly * rwj;
+          dsdt = Src[v] - (double)d * rJ;
+        }
         const long long gi = t + (long long)PP * (v + NV * e);
         if (a.mode == MODE_TENDENCY) {
           a.dSdt[gi] = dsdt;

@@ -143,6 +143,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   double* sdg = reinterpret_cast<double*>(smem + pl.oMats);
   double* sb = sdg + PP;
   double* sqw = sb + 2 * P;
+  double* sqwr = sqw + P;  // 1/w (used by the FP32-bulk form)
   volatile int* gflag = reinterpret_cast<volatile int*>(smem + pl.oFlags);
   unsigned char* slots = smem + pl.oSlots;
 
@@ -154,7 +155,10 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   // columns of its nodes' i (or j) are then consecutive
   for (int k = threadIdx.x; k < PP; k += blockDim.x) sdg[k] = a.dgM[k / P + P * (k % P)];
   for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) sb[k] = a.bM[k];
-  for (int k = threadIdx.x; k < P; k += blockDim.x) sqw[k] = a.qw[k];
+  for (int k = threadIdx.x; k < P; k += blockDim.x) {
+    sqw[k] = a.qw[k];
+    sqwr[k] = 1.0 / a.qw[k];
+  }
   __syncthreads();
   // Launched as a programmatic dependent of the previous kernel on the stream:
   // let the next launch start its own prologue, then wait until the previous
@@ -460,15 +464,28 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       double Src[NV], na[3];
       node_aux(na);
       Phys::template source<double>(qv, na, a, Src);
-      const R wi = (R)sqw[i], wj = (R)sqw[j];
       R d[NV];  // volume sums from phase B
 #pragma unroll
       for (int v = 0; v < NV; ++v) d[v] = gU[v * PP + t];
+      if constexpr (sizeof(R) == 8) {
+        // the reference's divisions, rounded as it rounds them (bit-exact form)
+        const R wi = (R)sqw[i], wj = (R)sqw[j];
 #pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        const R dv = d[v] + ((R)sb[i + P] * gfb[1 * SS + v * P + j] + (R)sb[i] * gfb[3 * SS + v * P + j]) / wi +
-                     ((R)sb[j + P] * gfb[2 * SS + v * P + i] + (R)sb[j] * gfb[0 * SS + v * P + i]) / wj;
-        dsdt[v] = Src[v] - (double)dv / Jij;
+        for (int v = 0; v < NV; ++v) {
+          const R dv = d[v] + ((R)sb[i + P] * gfb[1 * SS + v * P + j] + (R)sb[i] * gfb[3 * SS + v * P + j]) / wi +
+                       ((R)sb[j + P] * gfb[2 * SS + v * P + i] + (R)sb[j] * gfb[0 * SS + v * P + i]) / wj;
+          dsdt[v] = Src[v] - (double)dv / Jij;
+        }
+      } else {
+        // FP32 bulk: products with the reciprocals (one division per node)
+        const R rwi = (R)sqwr[i], rwj = (R)sqwr[j];
+        const double rJ = 1.0 / Jij;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          const R dv = d[v] + ((R)sb[i + P] * gfb[1 * SS + v * P + j] + (R)sb[i] * gfb[3 * SS + v * P + j]) * rwi +
+                       ((R)sb[j + P] * gfb[2 * SS + v * P + i] + (R)sb[j] * gfb[0 * SS + v * P + i]) * rwj;
+          dsdt[v] = Src[v] - (double)dv * rJ;
+        }
       }
     }
     named_bar(barId, TPE);  // every thread is done reading the flux array and the buffer
@@ -576,7 +593,7 @@ inline bool make_tma_plan(const StageArgs& a, int smemLimit, TmaPlan& pl, int ma
     s += 2 * C * 8;  // barriers
     s = (s + 15) / 16 * 16;
     const int oMats = s;
-    s += (PP + 3 * P) * 8;
+    s += (PP + 4 * P) * 8;  // dgMatrix, bMatrix, weights, reciprocal weights
     const int oFlags = s;
     s += C * 4;  // group flags
     s = (s + 127) / 128 * 128;
