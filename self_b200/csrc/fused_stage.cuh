@@ -221,7 +221,15 @@ struct PhysCIG {
   // The volume flux needs u, v, p and rhoH only (no sound speed).
   template <typename R>
   __device__ static void node_flux(R* f, const StageArgs& s) {
-    const R u = f[0] / f[2], v = f[1] / f[2];
+    R u, v;
+    if constexpr (sizeof(R) == 4) {  // FP32 bulk: one reciprocal of the density
+      const R r = (R)1 / f[2];
+      u = f[0] * r;
+      v = f[1] * r;
+    } else {
+      u = f[0] / f[2];
+      v = f[1] / f[2];
+    }
     const R ke = (R)0.5 * (f[0] * u + f[1] * v);
     const R p = ((R)s.gamma - (R)1) * (f[3] - ke);
     f[4] = u;

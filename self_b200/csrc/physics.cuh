@@ -80,12 +80,22 @@ __device__ __forceinline__ void sw_flux(R Hu, R Hv, R H, R u, R v, R g, R Fx[3],
 template <typename R>
 __device__ __forceinline__ void cig_state(R rhoU, R rhoV, R rho, R rhoE, R gamma, R& u, R& v, R& p, R& rhoKE,
                                           R& rhoH, R& c) {
-  u = rhoU / rho;
-  v = rhoV / rho;
-  rhoKE = (R)0.5 * (rhoU * u + rhoV * v);
-  p = (gamma - (R)1) * (rhoE - rhoKE);
-  rhoH = rhoE + p;
-  c = sqrt(gamma * p / rho);
+  if constexpr (sizeof(R) == 4) {  // FP32 bulk: one reciprocal of the density
+    const R r = (R)1 / rho;
+    u = rhoU * r;
+    v = rhoV * r;
+    rhoKE = (R)0.5 * (rhoU * u + rhoV * v);
+    p = (gamma - (R)1) * (rhoE - rhoKE);
+    rhoH = rhoE + p;
+    c = sqrt(gamma * p * r);
+  } else {  // the reference's divisions
+    u = rhoU / rho;
+    v = rhoV / rho;
+    rhoKE = (R)0.5 * (rhoU * u + rhoV * v);
+    p = (gamma - (R)1) * (rhoE - rhoKE);
+    rhoH = rhoE + p;
+    c = sqrt(gamma * p / rho);
+  }
 }
 
 // NaiveLLF, src/models/SELF_CompressibleIdealGas2D.f90:1486-1534.
