@@ -8,19 +8,22 @@ flux, Williamson RK3 at CFL 0.5 (dt from CovariantArcMin), 200 RK3 steps:
 one full solve.  Inputs are seeded synthetic fields of this shape (the
 reference ships no data for it).
 
-Reported (one JSON line on rank 0):
+Reported (one JSON line on rank 0), for the production FP64 form:
   value     DOF-updates/s with the state resident in HBM, device-timed with
             CUDA events on the engine's stream, L2 flushed before every solve
-  e2e       the same metric through the public API with host buffers: each
-            step copies the initial state host->device from pinned memory,
-            runs the solve, and copies the final state back
+  e2e       the same metric through the C ABI a Fortran caller uses, with
+            host buffers: each step copies the initial state from pinned host
+            memory into hipMalloc'd device buffers (the library's HIP memory
+            shim, as SELF's UpdateDevice does), runs the solve with
+            selfgpu_model2d_rk3 on the engine's default stream, and copies
+            the final state back with hipMemcpy (UpdateHost)
   roofline  algorithmic bytes per fused-stage launch / measured launch time
   cpu_baseline  the CPU oracle (C++ restatement of the reference CPU path,
             OpenMP over elements) on a bounded sample of the same workload
 
 ``--impl reference`` times the reference algorithm's CPU implementation (the
 oracle port; the Fortran reference cannot be built in this image) on the same
-workload, metric and unit.  Multi-GPU: the path runs as independent replicas
+workload, metric, unit, config and step definition (one 200-step solve).  Multi-GPU: the path runs as independent replicas
 (one per rank, no data-path collective); value = all ranks' DOF-updates over
 the slowest rank's time.
 """
@@ -46,6 +49,18 @@ DOF = NVAR * P * P * NEL
 GAMMA = 1.4
 WORKLOAD = (f"CompressibleIdealGas2D periodic {NX}x{NX} perturbed(0.02h) N={N} Gauss, FP64, naive LLF, "
             f"Williamson RK3 CFL {CFL}, {STEPS_PER_SOLVE} steps per solve")
+
+
+def cfl_dt(arcmin, rho_min):
+    """dt = CFL * ArcMin / max(|u| + c) of the initial state, c = sqrt(gamma p / rho), p = 1."""
+    return CFL * arcmin / (np.hypot(0.5, 0.3) + float(np.sqrt(GAMMA / rho_min)))
+
+
+def config_dict(dt, world):
+    """The config both arms print (same workload, same step definition)."""
+    return {"workload": WORKLOAD, "elements": NEL, "dof": DOF, "rk3_steps_per_step": STEPS_PER_SOLVE,
+            "dt": round(dt, 12), "parallelism": "replicas" if world > 1 else "single-gpu",
+            "l2": "flushed (256 MB write) before every timed solve; per-stage working set ~150 MB > L2"}
 
 
 def algorithmic_bytes_per_element_stage():
@@ -497,17 +512,17 @@ def measure_c5(mlp7, steps=100):
 
 
 def measure_c2_forms():
-    """C2 in the FP64 and FP32-bulk forms (smooth: no closure), FP32 error vs FP64."""
+    """C2 in the production FP64, reference-rounding FP64 and FP32-bulk forms
+    (smooth: no closure); relative L2 differences against the production FP64 run."""
     import self_b200 as S
     interp = S.Lagrange(N, S.GAUSS, N, S.UNIFORM)
     mesh = S.Mesh2D(NX, NX, periodic=(True, True), perturbation=0.02)
     geo = S.SEMQuad(interp, mesh)
     q0 = initial_state(geo.x)
-    c = (GAMMA * 1.0 / (q0[:, 2].min())).sqrt().item()
-    dt = CFL * geo.CovariantArcMin() / (np.hypot(0.5, 0.3) + c)
+    dt = cfl_dt(geo.CovariantArcMin(), q0[:, 2].min().item())
     c2 = {}
     ref2 = None
-    for name, form in (("fp64", S.FP64), ("fp32_bulk", S.FP32_BULK)):
+    for name, form in (("fp64", S.FP64), ("fp64_ref", S.FP64_REF), ("fp32_bulk", S.FP32_BULK)):
         res, sol = _closure_variant(mesh, geo, q0, form, S.CLOSURE_OFF, None, STEPS_PER_SOLVE, dt, DOF,
                                     nvtx=f"c2_{name}")
         if ref2 is None:
@@ -516,6 +531,7 @@ def measure_c2_forms():
             res["rel_l2_vs_fp64"] = _rel_l2(sol, ref2)
         c2[name] = res
     c2["speedup_fp32_bulk_vs_fp64"] = c2["fp32_bulk"]["value"] / c2["fp64"]["value"]
+    c2["speedup_fp64_vs_fp64_ref"] = c2["fp64"]["value"] / c2["fp64_ref"]["value"]
     return c2
 
 
@@ -582,26 +598,88 @@ def run_reference(args, rank, world):
     rho = 1 + 0.1 * np.sin(2 * np.pi * X) * np.sin(2 * np.pi * Y)
     q[:, :, 0], q[:, :, 1], q[:, :, 2] = rho * 0.5, rho * 0.3, rho
     q[:, :, 3] = 1 / (GAMMA - 1) + 0.5 * rho * 0.34
-    mod.set("solution", q)
-    dt = 1e-4
+    dt = cfl_dt(g.arcmin, float(rho.min()))
+
+    def solve():  # one step: the same full 200-step solve the GPU arm times
+        mod.set("solution", q)
+        mod.rk3(STEPS_PER_SOLVE, dt)
+
     for _ in range(args.warmup):
-        mod.rk3(1, dt)
+        solve()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        mod.rk3(1, dt)
+        solve()
     el = time.perf_counter() - t0
-    v = DOF * args.steps / el
-    sample = (f"each step = 1 RK3 step of the full {NX}x{NX} N={N} mesh (1/{STEPS_PER_SOLVE} of a solve); "
-              f"C++ restatement of the reference CPU path (the Fortran reference needs gfortran, hipfort, MPI and "
-              f"HDF5, none of which exist in this image)")
+    v = DOF * STEPS_PER_SOLVE * args.steps / el
+    sample = (f"each step = one full {STEPS_PER_SOLVE}-step RK3 solve of the {NX}x{NX} N={N} mesh, as on the GPU "
+              f"arm; C++ restatement of the reference CPU path, OpenMP over elements on {cores} host threads (the "
+              f"Fortran reference needs gfortran, hipfort, MPI and HDF5, none of which exist in this image)")
     print(json.dumps({
         "impl": "reference", "metric": "DOF-updates/s", "value": v, "unit": "DOF-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "elements": NEL, "dof": DOF, "parallelism": "replicas"},
+        "config": config_dict(dt, world),
         "cpu_baseline": {"value": v, "unit": "DOF-updates/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+def e2e_through_c_abi(S, mesh, geo, q0, dt, args):
+    """The solve as a Fortran caller runs it through the C ABI: device state
+    from the library's hipMalloc, UpdateDevice (hipMemcpy from pinned host
+    memory), selfgpu_model2d_rk3 on the handle's default (blocking) stream,
+    UpdateHost (hipMemcpy back).  Returns the device time of args.steps such
+    solves (CUDA events on the legacy default stream, which the copies and the
+    engine's blocking stream are ordered with) and the bytes copied per step."""
+    import torch
+    L = S.lib()
+    interp = geo.interp
+    h = ctypes.c_void_p()
+    S.check(L.selfgpu_model2d_create(ctypes.byref(h), S.MODEL_CIG, N, NEL, S.FP64, None))
+    mats = [np.asfortranarray(m) for m in (interp.dgMatrix, interp.bMatrix, interp.qWeights)]
+    S.check(L.selfgpu_model2d_set_interp(h, *[m.ctypes.data_as(ctypes.c_void_p) for m in mats]))
+    si = np.asfortranarray(mesh.sideInfo)
+    dp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    S.check(L.selfgpu_model2d_set_geometry(h, dp(geo.dsdx), dp(geo.J), dp(geo.nHat), dp(geo.nScale),
+                                           dp(mesh.sideInfo_d), si.ctypes.data_as(ctypes.c_void_p)))
+    S.check(L.selfgpu_model2d_set_params(h, 1.0, 0.0, GAMMA, 1.0))
+    host_q = torch.empty(q0.shape, dtype=torch.float64, pin_memory=True)
+    host_q.copy_(q0.cpu())
+    host_out = torch.empty_like(host_q).pin_memory()
+    nbytes = host_q.numel() * 8
+    d_q, d_g = ctypes.c_void_p(), ctypes.c_void_p()
+    if L.hipMalloc(ctypes.byref(d_q), nbytes) or L.hipMalloc(ctypes.byref(d_g), nbytes):
+        raise RuntimeError("hipMalloc failed")
+    zero = torch.zeros_like(host_q).pin_memory()
+    L.hipMemcpy(d_g, ctypes.c_void_p(zero.data_ptr()), nbytes, 1)  # the RK register starts at zero (H21)
+    S.check(L.selfgpu_model2d_set_state(h, d_q, d_g))
+
+    def solve():
+        if L.hipMemcpy(d_q, ctypes.c_void_p(host_q.data_ptr()), nbytes, 1):
+            raise RuntimeError("hipMemcpy H2D failed")
+        S.check(L.selfgpu_model2d_invalidate(h))
+        S.check(L.selfgpu_model2d_rk3(h, dt, STEPS_PER_SOLVE))
+        if L.hipMemcpy(ctypes.c_void_p(host_out.data_ptr()), d_q, nbytes, 2):
+            raise RuntimeError("hipMemcpy D2H failed")
+
+    for _ in range(max(1, args.warmup)):
+        solve()
+    S.check(L.selfgpu_model2d_sync(h))
+    from self_b200 import replicas as R
+    R.barrier()
+    leg = torch.cuda.default_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(leg)
+    for _ in range(args.steps):
+        solve()
+    e1.record(leg)
+    torch.cuda.synchronize()
+    S.check(L.selfgpu_model2d_check_finite(h))
+    S.check(L.selfgpu_model2d_destroy(h))
+    L.hipFree(d_q)
+    L.hipFree(d_g)
+    return e0.elapsed_time(e1), int(nbytes), int(nbytes)
 
 
 def run_engine(args, rank, world, local_rank):
@@ -618,9 +696,7 @@ def run_engine(args, rank, world, local_rank):
     S.lib().selfgpu_model2d_set_kernel(model._h, 1 if args.kernel == "persistent" else 0)
     q0 = initial_state(geo.x)
     torch.cuda.synchronize()
-    # CFL time step: dt = CFL * ArcMin / max(|u| + c)
-    c = (GAMMA * 1.0 / (q0[:, 2].min())).sqrt().item()
-    dt = CFL * geo.CovariantArcMin() / (np.hypot(0.5, 0.3) + c)
+    dt = cfl_dt(geo.CovariantArcMin(), q0[:, 2].min().item())
     flush = torch.empty(64 * 1024 * 1024, device=dev, dtype=torch.float32)  # 256 MB > 126 MB L2
 
     def solve():
@@ -664,32 +740,10 @@ def run_engine(args, rank, world, local_rank):
     peak, peak_kind = peaks()
     traffic = recorded_traffic()
 
-    # ---- end to end through the public API with host buffers
-    host_q = torch.empty(q0.shape, dtype=torch.float64, pin_memory=True)
-    host_q.copy_(q0.cpu())
-    host_out = torch.empty_like(host_q).pin_memory()
-    with torch.cuda.stream(stream):
-        for _ in range(max(1, args.warmup // 2)):
-            model.solution.copy_(host_q, non_blocking=True)
-            model.workSol.zero_()
-            S.lib().selfgpu_model2d_invalidate(model._h)
-            model.ForwardStep(STEPS_PER_SOLVE, dt)
-            host_out.copy_(model.solution, non_blocking=True)
-        stream.synchronize()
-        R.barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            model.solution.copy_(host_q, non_blocking=True)
-            model.workSol.zero_()
-            S.lib().selfgpu_model2d_invalidate(model._h)
-            model.ForwardStep(STEPS_PER_SOLVE, dt)
-            host_out.copy_(model.solution, non_blocking=True)
-        e1.record(stream)
-        stream.synchronize()
-    e2e_ms = R.max_over_ranks(e0.elapsed_time(e1))
-    e2e = R.aggregate_rate(DOF * STEPS_PER_SOLVE * args.steps, world, e2e_ms / 1e3)
     model.CheckFinite()
+    e2e_ms, h2d, d2h = e2e_through_c_abi(S, mesh, geo, q0, dt, args)
+    e2e_ms = R.max_over_ranks(e2e_ms)
+    e2e = R.aggregate_rate(DOF * STEPS_PER_SOLVE * args.steps, world, e2e_ms / 1e3)
 
     if rank != 0:
         return
@@ -697,11 +751,11 @@ def run_engine(args, rank, world, local_rank):
         "metric": "DOF-updates/s", "value": value, "unit": "DOF-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "elements": NEL, "dof": DOF, "rk3_steps_per_step": STEPS_PER_SOLVE,
-                   "dt": dt, "parallelism": "replicas" if world > 1 else "single-gpu",
-                   "l2": "flushed (256 MB write) before every timed solve; per-stage working set ~150 MB > L2"},
-        "e2e": {"value": e2e, "unit": "DOF-updates/s", "h2d_bytes_per_step": int(host_q.numel() * 8),
-                "d2h_bytes_per_step": int(host_out.numel() * 8)},
+        "config": config_dict(dt, world),
+        "form": "SELFGPU_FP64 (production FP64: multiply-add contraction, reciprocal products)",
+        "e2e": {"value": e2e, "unit": "DOF-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "path": "hipMemcpy (HIP shim) H2D from pinned host -> selfgpu_model2d_rk3 (C ABI, default "
+                        "stream) -> hipMemcpy D2H"},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind,

@@ -25,6 +25,7 @@
 #ifndef SELFGPU_H
 #define SELFGPU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -45,8 +46,11 @@ extern "C" {
 #define SELFGPU_MODEL_SW 2  /* ShallowWater,       src/models/SELF_ShallowWater.f90 */
 #define SELFGPU_MODEL_CIG 3 /* CompressibleIdealGas2D, src/models/SELF_CompressibleIdealGas2D.f90 */
 /* arithmetic forms of the fused path */
-#define SELFGPU_FP64 0       /* plain FP64 (parity form) */
+#define SELFGPU_FP64 0       /* plain FP64, production build: multiply-add contraction and reciprocal
+                                products (within FP64 round-off of the reference CPU path) */
 #define SELFGPU_FP32_BULK 1  /* FP32 flux/divergence, FP64 metrics/sources/RK accumulation */
+#define SELFGPU_FP64_REF 2   /* plain FP64 with the reference's roundings: no contraction, the
+                                reference's divisions and order; equals the FP64 CPU path bit for bit */
 /* largest polynomial degree the fused kernels are instantiated for */
 #define SELFGPU_MAX_N 7
 /* status codes */
@@ -238,7 +242,7 @@ int selfgpu_semquad_generate(int N, int nEl, const double* nodeCoords_d, const d
 typedef struct selfgpu_model2d selfgpu_model2d;
 
 /* Create an engine for `model` (SELFGPU_MODEL_*), degree N (1..SELFGPU_MAX_N),
- * nEl elements, arithmetic form SELFGPU_FP64 or SELFGPU_FP32_BULK, on `stream`
+ * nEl elements, arithmetic form SELFGPU_FP64, SELFGPU_FP64_REF or SELFGPU_FP32_BULK, on `stream`
  * (a cudaStream_t, NULL = legacy default stream).  Mirrors Model2D%Init
  * (src/SELF_Model2D.f90:142-178) minus the buffers the caller already owns. */
 int selfgpu_model2d_create(selfgpu_model2d** out, int model, int N, int nEl, int form, void* stream);
@@ -337,18 +341,22 @@ int selfgpu_model2d_inject_stall(selfgpu_model2d* m, int enable);
  * not allocate device memory (a host code that owns every device buffer and
  * forbids the library to allocate, a process under a fixed device-memory cap,
  * a call inside a solver step that must not stall or fail on cudaMalloc).
- * It computes the CompressibleIdealGas2D tendency dSdt exactly as
- * selfgpu_model2d_tendency does for a CIG handle with no gravity, drag or
- * prescribed-boundary fields (periodic or no-normal-flow sides), from
- * caller-owned device arrays in SELF's layouts (solution (P,P,4,nEl), dsdx,
- * J, nHat, nScale, sideInfo on the device plus a host copy of sideInfo for
- * validation) and host copies of dgMatrix, bMatrix and qWeights.  It calls
- * no allocator: its face-trace scratch is a file-scope device array of
- * SELFGPU_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
- * until exit; inputs needing more (above 7281 elements at N = 7, 14563 at
- * N = 3) are rejected with SELFGPU_ERR_ARG.  The first call on a device looks
- * up the array's address (make it before any stream capture).  All calls on
- * a device share the array: calls that overlap on the GPU race. */
+ * It computes the CompressibleIdealGas2D tendency dSdt bit for bit as
+ * selfgpu_model2d_tendency does for a SELFGPU_FP64_REF CIG handle with no
+ * gravity, drag or prescribed-boundary fields, from caller-owned device
+ * arrays in SELF's layouts (solution (P,P,4,nEl), dsdx, J, nHat, nScale,
+ * sideInfo on the device plus a host copy of sideInfo for validation) and
+ * host copies of dgMatrix, bMatrix and qWeights.  Sides must be periodic /
+ * interior (bcid 0) or NONORMALFLOW walls; any other physical side is
+ * rejected with SELFGPU_ERR_ARG.  There is no gravity or drag term (so g
+ * plays no part) and R only enters a diagnostic the tendency does not use.
+ * It calls no allocator: its face-trace scratch is a file-scope device array
+ * of SELFGPU_NOALLOC_SCRATCH_BYTES; inputs needing more (above 7281 elements
+ * at N = 7, 14563 at N = 3) are rejected with SELFGPU_ERR_ARG.  CUDA loads
+ * device code lazily, so the first call on a device reserves the array there
+ * (and looks up its address), and the device holds it until the process
+ * exits: make that first call during set-up, before any stream capture.  All
+ * calls on a device share the array: calls that overlap on the GPU race. */
 int selfgpu_cig2d_tendency_noalloc(const double* solution, double* dSdt, const double* dsdx, const double* J,
                                    const double* nHat, const double* nScale, const int* sideInfo_d,
                                    const int* sideInfo_h, const double* dgMatrix, const double* bMatrix,
@@ -482,6 +490,27 @@ int selfgpu_model2d_caches(selfgpu_model2d* m, void** traces, int* traceBlockByt
  * (device arrays; blockBytes a multiple of 4; blocks on the device). */
 int selfgpu_pack_blocks(const void* cache, const int* blocks, int n, int blockBytes, void* packed, void* stream);
 int selfgpu_unpack_blocks(const void* packed, const int* blocks, int n, int blockBytes, void* cache, void* stream);
+
+/* ============================================ 8. HIP runtime memory shim */
+
+/* The five HIP runtime entry points SELF's Fortran memory layer reaches
+ * through hipfort's bind(c) interfaces (src/SELF_Memory.f90:11-12 USE
+ * hipfort), implemented on the CUDA runtime so that layer runs unchanged
+ * without ROCm/HIP: link hipfort's interface modules against libselfgpu
+ * instead of the HIP runtime (never both in one process).  Return value:
+ * hipError_t (0 = hipSuccess; 1 invalid value, 2 out of memory, 100 no
+ * device, 101 invalid device, 999 any other failure). */
+/* replaces hipMalloc as bound by hipfort: Alloc_hfReal_r1 etc., src/SELF_Memory.f90:362 */
+int hipMalloc(void** ptr, size_t sizeBytes);
+/* replaces hipFree: Free_hfReal_r1 etc., src/SELF_Memory.f90:767-777 */
+int hipFree(void* ptr);
+/* replaces hipMemcpy: UpdateHost/UpdateDevice, src/SELF_Memory.f90:988-1033, :1295-1306;
+ * kind = hipMemcpyKind (0 host-host, 1 host-device, 2 device-host, 3 device-device, 4 default) */
+int hipMemcpy(void* dst, const void* src, size_t sizeBytes, int kind);
+/* replaces hipGetDeviceCount: GPUAvailable, src/SELF_Memory.f90:336-350; src/SELF_Mesh.f90:2043 */
+int hipGetDeviceCount(int* count);
+/* replaces hipSetDevice: rank-to-GPU binding, src/SELF_Mesh.f90:2050 */
+int hipSetDevice(int deviceId);
 
 #ifdef __cplusplus
 }

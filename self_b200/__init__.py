@@ -6,5 +6,5 @@ Lagrange / Mesh2D / SEMQuad / Model2D API over that library's C ABI.
 """
 from ._lib import SelfGpuError, check, exported_symbols, lib  # noqa: F401
 from .api import (BC_NONORMALFLOW, BC_PRESCRIBED, BC_RADIATION, CLOSURE_INDICATOR, CLOSURE_MLP,  # noqa: F401
-                  CLOSURE_OFF, FP32_BULK, FP64, GAUSS, GAUSS_LOBATTO, MODEL_CIG, MODEL_LSW, MODEL_SW, UNIFORM, CompressibleIdealGas2D, Lagrange,
+                  CLOSURE_OFF, FP32_BULK, FP64, FP64_REF, GAUSS, GAUSS_LOBATTO, MODEL_CIG, MODEL_LSW, MODEL_SW, UNIFORM, CompressibleIdealGas2D, Lagrange,
                   LinearShallowWater, Mesh2D, Model2D, SEMQuad, ShallowWater, to_device, to_host)

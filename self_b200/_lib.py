@@ -77,6 +77,12 @@ _SIGS = {
                                        ctypes.POINTER(c_void_p), ctypes.POINTER(c_int)]),
     "selfgpu_pack_blocks": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p]),
     "selfgpu_unpack_blocks": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p]),
+    # HIP runtime memory shim (hipfort's bind(c) targets)
+    "hipMalloc": (c_int, [ctypes.POINTER(c_void_p), ctypes.c_size_t]),
+    "hipFree": (c_int, [c_void_p]),
+    "hipMemcpy": (c_int, [c_void_p, c_void_p, ctypes.c_size_t, c_int]),
+    "hipGetDeviceCount": (c_int, [ctypes.POINTER(c_int)]),
+    "hipSetDevice": (c_int, [c_int]),
     # drop-in wrappers (src/hip/*.cpp, src/models/hip/*.cpp of the reference)
     "ScalarGridInterp_2D_gpu_wrapper": (None, [PP, PP, PP, c_int, c_int, c_int, c_int]),
     "VectorGridInterp_2D_gpu_wrapper": (None, [PP, PP, PP, c_int, c_int, c_int, c_int]),

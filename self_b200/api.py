@@ -22,7 +22,9 @@ from ._lib import check, lib, pp
 GAUSS, GAUSS_LOBATTO, UNIFORM = 1, 2, 5
 BC_PRESCRIBED, BC_RADIATION, BC_NONORMALFLOW = 100, 101, 102
 MODEL_LSW, MODEL_SW, MODEL_CIG = 1, 2, 3
-FP64, FP32_BULK = 0, 1
+# arithmetic forms: FP64 = production FP64 (contraction, reciprocal products),
+# FP32_BULK = FP32 fluxes/divergence, FP64_REF = FP64 with the reference's roundings
+FP64, FP32_BULK, FP64_REF = 0, 1, 2
 
 
 def to_device(a, dtype=torch.float64, device="cuda"):

@@ -12,11 +12,13 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libselfgpu.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
-# (source, extra flags): the FP64 kernels are built without multiply-add
-# contraction so their roundings follow the reference's CPU path exactly.
+# (source, extra flags): the reference-rounding FP64 kernels (drop-in wrappers,
+# the SELFGPU_FP64_REF stage form, the FP64 closure) are built without
+# multiply-add contraction so their roundings follow the reference's CPU path
+# exactly; the production FP64 stage form (stage_fp64_prod.cu) contracts.
 SOURCES = [("setup_host.cpp", []), ("legacy_ops.cu", ["-fmad=false"]), ("stage_fp64.cu", ["-fmad=false"]),
-           ("stage_fp32.cu", []), ("engine.cu", []), ("noalloc.cu", ["-fmad=false"]), ("mlp.cu", []),
-           ("checkpoint.cpp", []), ("decomp.cpp", [])]
+           ("stage_fp64_prod.cu", []), ("stage_fp32.cu", []), ("engine.cu", []), ("noalloc.cu", ["-fmad=false"]),
+           ("mlp.cu", []), ("checkpoint.cpp", []), ("decomp.cpp", []), ("hip_shim.cpp", [])]
 HEADERS = ["selfgpu_internal.h", "physics.cuh", "fused_stage.cuh", "fused_stage_tma.cuh", "stage_dispatch.cuh",
            "av_closure.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

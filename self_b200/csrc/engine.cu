@@ -34,10 +34,12 @@ __global__ void k_nonfinite(const double* __restrict__ q, long long n, int* flag
 
 // One element's packed geometry record (geo_record_doubles<P>() doubles):
 // dsdx (4 P^2, two planes of per-node pairs), nHat (8 P), nScale (4 P), J (P^2),
-// then sideInfo's 20 ints.
+// then sideInfo's 20 ints.  invJ = 1 stores 1/J in J's place (the forms that
+// multiply by the reciprocal instead of dividing by J).
 __global__ void k_pack_geometry(const double* __restrict__ dsdx, const double* __restrict__ nHat,
                                 const double* __restrict__ nScale, const double* __restrict__ J,
-                                const int* __restrict__ sideInfo, int P, int nEl, int rec, double* __restrict__ out) {
+                                const int* __restrict__ sideInfo, int P, int nEl, int rec, int invJ,
+                                double* __restrict__ out) {
   const int PP = P * P;
   const long long total = (long long)rec * nEl;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
@@ -52,7 +54,7 @@ __global__ void k_pack_geometry(const double* __restrict__ dsdx, const double* _
     } else if ((w -= 8 * P) < 4 * P) {
       v = nScale[4 * P * e + w];
     } else if ((w -= 4 * P) < PP) {
-      v = J[PP * e + w];
+      v = invJ ? 1.0 / J[PP * e + w] : J[PP * e + w];
     } else {
       w -= PP;  // sideInfo: two ints per double slot
       int2 pr = make_int2(sideInfo[20 * e + 2 * w], sideInfo[20 * e + 2 * w + 1]);
@@ -115,7 +117,17 @@ struct selfgpu_model2d {
   float* mlpB = nullptr;
   double* geo = nullptr;  // packed geometry records (persistent kernel)
 
-  size_t elemBytes() const { return form == SELFGPU_FP64 ? sizeof(double) : sizeof(float); }
+  size_t elemBytes() const { return form == SELFGPU_FP32_BULK ? sizeof(float) : sizeof(double); }
+
+  // stage kernels of this handle's arithmetic form
+  static cudaError_t launch_stage_form(int form, int model, int P, const StageArgs& a, const StageLaunch& L,
+                                       cudaStream_t st, int* usedTma) {
+    switch (form) {
+      case SELFGPU_FP64: return launch_stage_fp64(model, P, a, L, st, usedTma);
+      case SELFGPU_FP64_REF: return launch_stage_fp64_ref(model, P, a, L, st, usedTma);
+      default: return launch_stage_fp32(model, P, a, L, st, usedTma);
+    }
+  }
 
   // closure preparation of one stage: element viscosity, BR1 gradient, viscous
   // volume flux and traces, from the solution and the trace cache trIn
@@ -132,8 +144,8 @@ struct selfgpu_model2d {
     x.presc = base.fld[2];
     x.gamma = base.gamma;
     launches += 2;
-    return form == SELFGPU_FP64 ? launch_av_prep_fp64(P, x, stream, cfg.numSMs)
-                                : launch_av_prep_fp32(P, x, stream, cfg.numSMs);
+    return form == SELFGPU_FP32_BULK ? launch_av_prep_fp32(P, x, stream, cfg.numSMs)
+                                     : launch_av_prep_fp64(P, x, stream, cfg.numSMs);
   }
 
   cudaError_t launch(StageArgs a) {
@@ -143,8 +155,7 @@ struct selfgpu_model2d {
     }
     ++launches;
     int tma = 0;
-    cudaError_t e = form == SELFGPU_FP64 ? launch_stage_fp64(model, P, a, cfg, stream, &tma)
-                                         : launch_stage_fp32(model, P, a, cfg, stream, &tma);
+    cudaError_t e = launch_stage_form(form, model, P, a, cfg, stream, &tma);
     tmaLaunches += tma;
     return e;
   }
@@ -233,7 +244,7 @@ int selfgpu_model2d_create(selfgpu_model2d** out, int model, int N, int nEl, int
   if (N < 1 || N > SELFGPU_MAX_N)
     return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_create: degree N must be in 1.." + std::to_string(SELFGPU_MAX_N));
   if (nEl < 1) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_create: nEl must be >= 1");
-  if (form != SELFGPU_FP64 && form != SELFGPU_FP32_BULK)
+  if (form != SELFGPU_FP64 && form != SELFGPU_FP64_REF && form != SELFGPU_FP32_BULK)
     return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_create: unknown arithmetic form");
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -336,7 +347,8 @@ int selfgpu_model2d_set_geometry(selfgpu_model2d* m, const double* dsdx, const d
   if (e == cudaSuccess) {
     const long long total = (long long)rec * m->nEl;
     const int blocks = (int)((total + 255) / 256 < 4096 ? (total + 255) / 256 : 4096);
-    k_pack_geometry<<<blocks, 256, 0, 0>>>(dsdx, nHat, nScale, J, sideInfo_d, P, m->nEl, rec, m->geo);
+    k_pack_geometry<<<blocks, 256, 0, 0>>>(dsdx, nHat, nScale, J, sideInfo_d, P, m->nEl, rec,
+                                           m->form != SELFGPU_FP64_REF, m->geo);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(0);
@@ -606,14 +618,12 @@ int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, f
     }
     m->cfg = c;
     int tma = 0;
-    e = (m->form == SELFGPU_FP64) ? launch_stage_fp64(m->model, m->P, a, c, m->stream, &tma)
-                                  : launch_stage_fp32(m->model, m->P, a, c, m->stream, &tma);
+    e = selfgpu_model2d::launch_stage_form(m->form, m->model, m->P, a, c, m->stream, &tma);
     if (e != cudaSuccess) break;
     if (cand > 0 && !tma) break;  // the persistent kernel does not apply
     cudaEventRecord(t0, m->stream);
     for (int r = 0; r < 3; ++r)
-      (m->form == SELFGPU_FP64) ? launch_stage_fp64(m->model, m->P, a, c, m->stream, &tma)
-                                : launch_stage_fp32(m->model, m->P, a, c, m->stream, &tma);
+      selfgpu_model2d::launch_stage_form(m->form, m->model, m->P, a, c, m->stream, &tma);
     cudaEventRecord(t1, m->stream);
     cudaEventSynchronize(t1);
     float ms = 0.f;

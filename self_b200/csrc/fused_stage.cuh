@@ -123,6 +123,7 @@ __host__ __device__ constexpr int trace_side_stride() {
 //   LSW  a = (H, fCori)            x = (H.boundary)
 //   SW   a = (dh/dx, dh/dy)        x = (topography.boundary)
 //   CIG  a = (gx, gy, Cd)          x = prescribed (rhoU,rhoV,rho,rhoE,u,v,p,rhoH,c)
+inline namespace SELFGPU_FORM_NS {
 struct PhysLSW {
   static constexpr int NV = 3, NT = 3, NF = 3;
   static constexpr bool kLaggedVelocity = false;
@@ -168,8 +169,14 @@ struct PhysSW {
   template <typename R>
   __device__ static void node(R* f, const StageArgs&) {
     const R H = f[2];  // src/models/SELF_ShallowWater.f90:205-216
-    f[3] = f[0] / H;
-    f[4] = f[1] / H;
+    if constexpr (ref_rounding<R>()) {
+      f[3] = f[0] / H;
+      f[4] = f[1] / H;
+    } else {
+      const R r = (R)1 / H;
+      f[3] = f[0] * r;
+      f[4] = f[1] * r;
+    }
   }
   template <typename R>
   __device__ static void node_flux(R* f, const StageArgs& s) {
@@ -222,7 +229,7 @@ struct PhysCIG {
   template <typename R>
   __device__ static void node_flux(R* f, const StageArgs& s) {
     R u, v;
-    if constexpr (sizeof(R) == 4) {  // FP32 bulk: one reciprocal of the density
+    if constexpr (!ref_rounding<R>()) {  // FP32 bulk / production FP64: one reciprocal of the density
       const R r = (R)1 / f[2];
       u = f[0] * r;
       v = f[1] * r;
@@ -270,6 +277,8 @@ struct PhysCIG {
     cig_llf<R>(L, X, n1, n2, nmag, out);
   }
 };
+
+}  // namespace SELFGPU_FORM_NS
 
 // Model fields from global memory (v1 kernel).  t = node, e = element.
 template <class Phys>
@@ -528,7 +537,8 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
       Phys::template source<double>(qd, na, a, Src);
       const double Jij = a.J[gnode];
       const R wi = (R)srw[i], wj = (R)srw[j];
-      // FP32 bulk: products with the reciprocals (the FP64 form divides as the reference does)
+      // FP32 bulk and production FP64: products with the reciprocals (the
+      // reference-rounding FP64 build divides as the reference does)
       const R rwi = (R)(1.0 / srw[i]), rwj = (R)(1.0 / srw[j]);
       const double rJ = 1.0 / Jij;
 #pragma unroll
@@ -540,7 +550,7 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
         const R lx = (R)sb[i + P] * sm.fb[1][v][j] + (R)sb[i] * sm.fb[3][v][j];
         const R ly = (R)sb[j + P] * sm.fb[2][v][i] + (R)sb[j] * sm.fb[0][v][i];
         double dsdt;
-        if constexpr (sizeof(R) == 8) {
+        if constexpr (ref_rounding<R>()) {
           d = d + lx / wi + ly / wj;
           dsdt = Src[v] - (double)d / Jij;
         } else {

@@ -459,6 +459,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       }
 #pragma unroll
       for (int v = 0; v < NV; ++v) qv[v] = sq[t + PP * v];
+      // J of the node (reference-rounding build) or 1/J (the other forms)
       const double Jij = reinterpret_cast<const double*>(sl + pl.oJ)[t];
       // sources in FP64 in every form (well-balanced topography / gravity terms)
       double Src[NV], na[3];
@@ -467,7 +468,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       R d[NV];  // volume sums from phase B
 #pragma unroll
       for (int v = 0; v < NV; ++v) d[v] = gU[v * PP + t];
-      if constexpr (sizeof(R) == 8) {
+      if constexpr (ref_rounding<R>()) {
         // the reference's divisions, rounded as it rounds them (bit-exact form)
         const R wi = (R)sqw[i], wj = (R)sqw[j];
 #pragma unroll
@@ -477,9 +478,10 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
           dsdt[v] = Src[v] - (double)dv / Jij;
         }
       } else {
-        // FP32 bulk: products with the reciprocals (one division per node)
+        // FP32 bulk and production FP64: products with the reciprocals of the
+        // weights; the packed record of these forms holds 1/J in J's place
         const R rwi = (R)sqwr[i], rwj = (R)sqwr[j];
-        const double rJ = 1.0 / Jij;
+        const double rJ = Jij;
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
           const R dv = d[v] + ((R)sb[i + P] * gfb[1 * SS + v * P + j] + (R)sb[i] * gfb[3 * SS + v * P + j]) * rwi +

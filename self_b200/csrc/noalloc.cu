@@ -8,21 +8,30 @@
 // limit, a pool reserved for one solver), or a call site deep inside a solver
 // step that must not stall or fail on cudaMalloc.  For them this file keeps
 // the scratch it needs -- the face-trace buffer written by one launch and read
-// by the next -- in a fixed, file-scope device array that is loaded with the
-// library.  The caller still passes every input and output buffer.
+// by the next -- in a fixed, file-scope device array of the library's device
+// code.  The caller still passes every input and output buffer.
 //
 // Costs and limits of that choice:
-//  * every GPU that loads the library holds SELFGPU_NOALLOC_SCRATCH_BYTES
-//    (16 MiB) of device memory for this array until the process exits;
+//  * every GPU on which the entry point has been called holds
+//    SELFGPU_NOALLOC_SCRATCH_BYTES (16 MiB) of device memory for this array
+//    until the process exits;
 //  * the array is shared by all calls on a device: two calls whose launches
 //    overlap on the GPU (different streams, or different host threads) race
 //    on it and produce wrong results -- serialise them;
 //  * the array keeps the last call's contents.  Nothing in it needs to start
 //    at zero: the first launch of each call writes every entry the second
 //    launch reads;
-//  * the first call on a device resolves the array's device address with
-//    cudaGetSymbolAddress (with that device current); make that first call
-//    before any stream capture that is to contain later calls.
+//  * CUDA loads a module's device code lazily by default, so the array is
+//    reserved on a device by the first call there (its address lookup), not
+//    when the library is loaded: make one call on each device during set-up,
+//    before any stream capture that is to contain later calls.  The first
+//    call resolves the array's device address with cudaGetSymbolAddress
+//    (with that device current); a failed lookup is not kept, the next call
+//    tries again;
+//  * the tendency has no gravity, drag or prescribed-boundary fields: sides
+//    are periodic / interior (bcid 0) or NONORMALFLOW walls, and any other
+//    physical side (PRESCRIBED, RADIATION, ...) is rejected, since its
+//    exterior state would be zero (zero density) here.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -41,20 +50,25 @@ constexpr int kMaxDevices = 64;
 // Values per (element, side) block of the CompressibleIdealGas2D FP64 trace
 // layout: 9 traced fields x P nodes, padded to 16 bytes.
 int trace_block(int N) { return (9 * (N + 1) + 1) / 2 * 2; }
-std::once_flag g_once[kMaxDevices];
+std::mutex g_scratch_mutex;
 void* g_scratch_ptr[kMaxDevices] = {};
-cudaError_t g_scratch_err[kMaxDevices] = {};
 
-// Device address of the scratch array on `dev` (the current device).
+// Device address of the scratch array on `dev` (the current device).  Only a
+// successful lookup is kept; after a failure (for instance a first call made
+// during stream capture) the next call looks it up again.
 cudaError_t scratch_address(int dev, void** out) {
-  std::call_once(g_once[dev], [dev] {
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (g_scratch_ptr[dev] == nullptr) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    g_scratch_ptr[dev] = (e == cudaSuccess) ? p : nullptr;
-    g_scratch_err[dev] = e;
-  });
+    if (e != cudaSuccess || p == nullptr) {
+      *out = nullptr;
+      return e != cudaSuccess ? e : cudaErrorInvalidSymbol;
+    }
+    g_scratch_ptr[dev] = p;
+  }
   *out = g_scratch_ptr[dev];
-  return g_scratch_err[dev];
+  return cudaSuccess;
 }
 
 template <int P>
@@ -107,6 +121,17 @@ extern "C" int selfgpu_cig2d_tendency_noalloc(const double* solution, double* dS
     return set_error(SELFGPU_ERR_ARG, "selfgpu_cig2d_tendency_noalloc: dsdx and nHat must be 16-byte aligned");
   int rc = validate_side_info(sideInfo_h, nEl, nEl);
   if (rc != SELFGPU_OK) return rc;
+  // physical sides (no neighbour element) must be NONORMALFLOW walls: there
+  // are no prescribed traces here, and any other boundary condition would see
+  // a zero exterior state
+  for (long long k = 0; k < 4LL * nEl; ++k) {
+    const int* si = sideInfo_h + 5 * k;
+    if (si[2] == 0 && si[4] != 0 && si[4] != SELFGPU_BC_NONORMALFLOW)
+      return set_error(SELFGPU_ERR_ARG, "selfgpu_cig2d_tendency_noalloc: side " + std::to_string(k % 4 + 1) +
+                                            " of element " + std::to_string(k / 4 + 1) + " has boundary condition " +
+                                            std::to_string(si[4]) +
+                                            "; only periodic/interior sides and NONORMALFLOW walls are supported");
+  }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
@@ -127,8 +152,8 @@ extern "C" int selfgpu_cig2d_tendency_noalloc(const double* solution, double* dS
   a.dSdt = dSdt;
   a.trOut = scratch;
   a.gamma = expansionFactor;
-  a.g = 1.0;
-  a.Rgas = 1.0;
+  a.g = 1.0;     // no gravity field is bound, so g never enters the tendency
+  a.Rgas = 1.0;  // the gas constant only enters the (unused) temperature diagnostic
   for (int k = 0; k < P * P; ++k) a.dgM[k] = dgMatrix[k];
   for (int k = 0; k < 2 * P; ++k) a.bM[k] = bMatrix[k];
   for (int k = 0; k < P; ++k) a.qw[k] = qWeights[k];

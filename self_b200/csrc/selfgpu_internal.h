@@ -25,7 +25,7 @@ int validate_side_info(const int* sideInfo, int nEl, int nNeighbours);
 // T(k,i) = w_i sqrt((2k+1)/2) L_k(x_i): nodal -> orthonormal Legendre modes
 void modal_matrix(int N, const double* x, const double* w, double* T);
 
-// Fused stage launches (stage_fp64.cu / stage_fp32.cu).
+// Fused stage launches (stage_fp64_prod.cu / stage_fp64.cu / stage_fp32.cu).
 struct StageArgs;
 struct StageLaunch {
   bool allowTma;   // use the persistent bulk-copy kernel where it applies
@@ -38,8 +38,11 @@ struct StageLaunch {
 #include <cuda_runtime.h>
 
 namespace selfgpu {
+// production FP64 (stage_fp64_prod.cu), reference roundings (stage_fp64.cu), FP32 bulk
 cudaError_t launch_stage_fp64(int model, int P, const StageArgs& a, const StageLaunch& L, cudaStream_t st,
                               int* usedTma);
+cudaError_t launch_stage_fp64_ref(int model, int P, const StageArgs& a, const StageLaunch& L, cudaStream_t st,
+                                  int* usedTma);
 cudaError_t launch_stage_fp32(int model, int P, const StageArgs& a, const StageLaunch& L, cudaStream_t st,
                               int* usedTma);
 // Artificial-viscosity closure (av_closure.cuh).

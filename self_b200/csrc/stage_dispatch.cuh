@@ -1,6 +1,8 @@
 // Host-side launch of the fused stage kernels for one bulk type R.  Included
 // by stage_fp64.cu (built with -fmad=false so that every FP64 operation rounds
-// exactly as the reference's CPU path does) and stage_fp32.cu.
+// exactly as the reference's CPU path does), stage_fp64_prod.cu (the
+// production FP64 form) and stage_fp32.cu.  The launchers sit in the build's
+// form namespace (physics.cuh), so each build launches its own kernels.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -13,6 +15,7 @@
 #include "selfgpu_internal.h"
 
 namespace selfgpu {
+inline namespace SELFGPU_FORM_NS {
 
 template <int P, class Phys, typename R>
 constexpr int elems_per_block() {
@@ -96,4 +99,5 @@ cudaError_t launch_stage_impl(int model, int P, const StageArgs& a, const StageL
   }
 }
 
+}  // namespace SELFGPU_FORM_NS
 }  // namespace selfgpu

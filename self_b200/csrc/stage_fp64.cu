@@ -1,4 +1,5 @@
-// FP64 instantiation of the fused stage kernels.  Built with -fmad=false: no
+// Reference-rounding FP64 instantiation of the fused stage kernels (form
+// SELFGPU_FP64_REF) and the FP64 closure kernels.  Built with -fmad=false: no
 // multiply-add contraction, and divisions and square roots are IEEE correctly
 // rounded, so each value is formed with the same roundings as the reference's
 // FP64 CPU path evaluated in the same order.
@@ -6,8 +7,8 @@
 #include "stage_dispatch.cuh"
 
 namespace selfgpu {
-cudaError_t launch_stage_fp64(int model, int P, const StageArgs& a, const StageLaunch& L, cudaStream_t st,
-                              int* usedTma) {
+cudaError_t launch_stage_fp64_ref(int model, int P, const StageArgs& a, const StageLaunch& L, cudaStream_t st,
+                                  int* usedTma) {
   return launch_stage_impl<double>(model, P, a, L, st, usedTma);
 }
 

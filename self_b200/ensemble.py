@@ -162,12 +162,12 @@ class UnbatchedShallowWater:
     """The same instances advanced one handle per instance, sequentially: the
     plain FP64 GPU form an ensemble is compared against."""
 
-    def __init__(self, instances, g=1.0):
+    def __init__(self, instances, g=1.0, form=A.FP64):
         self.runs = []
         for inst in instances:
             mesh = A.Mesh2D(inst.nx, inst.ny, bcid=A.BC_NONORMALFLOW)
             geo = A.SEMQuad(A.Lagrange(inst.N), mesh)
-            model = A.ShallowWater(mesh, geo, form=A.FP64)
+            model = A.ShallowWater(mesh, geo, form=form)
             model.g = g
             model._push_params()
             X, Y = geo.x[:, 0, :, :, 0], geo.x[:, 0, :, :, 1]

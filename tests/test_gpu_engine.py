@@ -1,9 +1,12 @@
 """Parity of the fused CUDA engine (libselfgpu) with the FP64 CPU oracle.
 
 Tolerance: 1e-12 relative (max abs difference over max abs reference value,
-per field) for the tendency and after RK3 steps -- the bar the FP64 form is
-held to.  Every case runs the reference's call order: mesh -> geometry ->
-model fields -> SetSolution -> CalculateTendency / ForwardStep.
+per field) for the tendency and after RK3 steps -- the bar both FP64 forms
+are held to: the production form (FP64, multiply-add contraction and
+reciprocal products) and the reference-rounding form (FP64_REF), which in
+addition equals the oracle bit for bit.  Every case runs the reference's call
+order: mesh -> geometry -> model fields -> SetSolution -> CalculateTendency /
+ForwardStep.
 """
 import numpy as np
 import pytest
@@ -14,9 +17,10 @@ from tests import cases as C
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
+FORMS = [0, 2]  # self_b200.FP64 (production), self_b200.FP64_REF (reference roundings)
 
 
-def build_pair(model, mesh_kind, N, seed=0):
+def build_pair(model, mesh_kind, N, seed=0, form=0):
     import self_b200 as S
     kw = C.mesh_kwargs(mesh_kind)
     om, pm = C.oracle_mesh(kw), C.product_mesh(kw)
@@ -25,7 +29,7 @@ def build_pair(model, mesh_kind, N, seed=0):
     interp = S.Lagrange(N, S.GAUSS, N, S.UNIFORM)
     geo = S.SEMQuad(interp, pm)
     cls = {"LSW": S.LinearShallowWater, "SW": S.ShallowWater, "CIG": S.CompressibleIdealGas2D}[model]
-    mod = cls(pm, geo)
+    mod = cls(pm, geo, form=form)
     aux = C.aux_fields(model, geo_o.x, seed)
     if model == "LSW":
         mod_o.set("H", aux["H"])
@@ -66,11 +70,12 @@ CASES = [(m, k) for m in ("LSW", "SW", "CIG") for k in ("periodic", "walls", "fl
         [("CIG", "prescribed")]
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("N", [2, 3, 4, 7])  # odd and even P; P*P < 4P at N = 2
 @pytest.mark.parametrize("model,mesh_kind", CASES)
-def test_tendency_matches_oracle(model, mesh_kind, N):
+def test_tendency_matches_oracle(model, mesh_kind, N, form):
     import self_b200 as S
-    mod_o, mod, _, _ = build_pair(model, mesh_kind, N)
+    mod_o, mod, _, _ = build_pair(model, mesh_kind, N, form=form)
     ref = mod_o.tendency()
     got = S.to_host(mod.CalculateTendency()).reshape(ref.shape, order="F")
     for v in range(ref.shape[2]):
@@ -84,28 +89,30 @@ def test_tendency_matches_oracle(model, mesh_kind, N):
 @pytest.mark.parametrize("model,mesh_kind", [("LSW", "walls"), ("SW", "flipped"), ("CIG", "periodic"),
                                              ("CIG", "prescribed")])
 def test_fp64_tendency_and_steps_are_bit_exact(model, mesh_kind):
-    """The FP64 form evaluates every expression in the reference's order with
-    IEEE roundings and no multiply-add contraction, on geometry built the same
-    way: tendency and RK3 states equal the oracle's bit for bit."""
+    """The reference-rounding FP64 form evaluates every expression in the
+    reference's order with IEEE roundings and no multiply-add contraction, on
+    geometry built the same way: tendency and RK3 states equal the oracle's
+    bit for bit."""
     import self_b200 as S
     N = 7
-    mod_o, mod, _, _ = build_pair(model, mesh_kind, N, seed=2)
+    mod_o, mod, _, _ = build_pair(model, mesh_kind, N, seed=2, form=S.FP64_REF)
     ref = mod_o.tendency()
     got = S.to_host(mod.CalculateTendency()).reshape(ref.shape, order="F")
     np.testing.assert_array_equal(got, ref)
-    mod_o2, mod2, _, _ = build_pair(model, mesh_kind, N, seed=2)
+    mod_o2, mod2, _, _ = build_pair(model, mesh_kind, N, seed=2, form=S.FP64_REF)
     mod_o2.rk3(4, 1e-3)
     mod2.ForwardStep(4, 1e-3)
     ref = mod_o2.get("solution", ref.shape)
     np.testing.assert_array_equal(S.to_host(mod2.solution).reshape(ref.shape, order="F"), ref)
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("N", [2, 5])
 @pytest.mark.parametrize("model,mesh_kind", CASES)
-def test_rk3_steps_match_oracle(model, mesh_kind, N):
+def test_rk3_steps_match_oracle(model, mesh_kind, N, form):
     import self_b200 as S
     n, dt = 12, 1e-3
-    mod_o, mod, _, _ = build_pair(model, mesh_kind, N, seed=3)
+    mod_o, mod, _, _ = build_pair(model, mesh_kind, N, seed=3, form=form)
     mod_o.rk3(n, dt)
     mod.ForwardStep(n, dt)
     ref = mod_o.get("solution", (N + 1, N + 1, mod.nVar, mod.nElem))
@@ -114,12 +121,13 @@ def test_rk3_steps_match_oracle(model, mesh_kind, N):
         assert C.rel_err(got[:, :, v], ref[:, :, v]) < TOL, (v, C.rel_err(got[:, :, v], ref[:, :, v]))
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("model", ["LSW", "SW", "CIG"])
-def test_100_rk3_steps_match_oracle(model):
+def test_100_rk3_steps_match_oracle(model, form):
     import self_b200 as S
     N, dt = 7, 5e-4
     mesh_kind = "periodic" if model == "CIG" else "walls"
-    mod_o, mod, _, _ = build_pair(model, mesh_kind, N, seed=7)
+    mod_o, mod, _, _ = build_pair(model, mesh_kind, N, seed=7, form=form)
     mod_o.rk3(100, dt)
     mod.ForwardStep(40, dt)  # split calls: graph replay across calls keeps the state
     mod.ForwardStep(60, dt)
@@ -130,31 +138,42 @@ def test_100_rk3_steps_match_oracle(model):
     mod.CheckFinite()
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("N", [4, 7])  # the per-element kernel (odd P) and the persistent kernel
 @pytest.mark.parametrize("model", ["LSW", "SW", "CIG"])
 @pytest.mark.parametrize("mesh_kind", ["single", "column", "row", "pair", "ring", "torus"])
-def test_edge_meshes_bit_exact(model, mesh_kind, N):
+def test_edge_meshes(model, mesh_kind, N, form):
     """Meshes at the edges of the layout: one element (all four sides
     physical), one column and one row of elements (fewer elements than SMs,
     so fewer CTAs than the persistent grid), the smallest periodic mesh,
     where each element is the neighbour of another on two sides and rotated
     elements meet with flipped sides, and periodic directions one element
     wide, where a side's neighbour is its own element.  Tendency and RK3
-    steps equal the oracle's bit for bit."""
+    steps equal the oracle's bit for bit in the reference-rounding form and
+    within 1e-12 in the production form."""
     import self_b200 as S
-    mod_o, mod, _, _ = build_pair(model, mesh_kind, N, seed=5)
+
+    def same(got, ref):
+        if form == S.FP64_REF:
+            np.testing.assert_array_equal(got, ref)
+        else:
+            for v in range(ref.shape[2]):
+                assert C.rel_err(got[:, :, v], ref[:, :, v]) < TOL, (v, C.rel_err(got[:, :, v], ref[:, :, v]))
+
+    mod_o, mod, _, _ = build_pair(model, mesh_kind, N, seed=5, form=form)
     ref = mod_o.tendency()
     got = S.to_host(mod.CalculateTendency()).reshape(ref.shape, order="F")
     assert np.isfinite(ref).all()
-    np.testing.assert_array_equal(got, ref)
-    mod_o2, mod2, _, _ = build_pair(model, mesh_kind, N, seed=5)
+    same(got, ref)
+    mod_o2, mod2, _, _ = build_pair(model, mesh_kind, N, seed=5, form=form)
     mod_o2.rk3(5, 1e-3)
     mod2.ForwardStep(5, 1e-3)
     ref = mod_o2.get("solution", ref.shape)
-    np.testing.assert_array_equal(S.to_host(mod2.solution).reshape(ref.shape, order="F"), ref)
+    same(S.to_host(mod2.solution).reshape(ref.shape, order="F"), ref)
 
 
-def test_c2_full_size_tendency_and_steps():
+@pytest.mark.parametrize("form", FORMS)
+def test_c2_full_size_tendency_and_steps(form):
     """The CompressibleIdealGas2D benchmark workload at full size: periodic
     128x128, perturbed nodes (0.02 h), N = 7: tendency and 2 RK3 steps against
     the oracle, plus free-stream preservation and discrete conservation."""
@@ -168,7 +187,7 @@ def test_c2_full_size_tendency_and_steps():
     geo_o = O.Geometry(N, om)
     mod_o = O.Model(O.CIG, N, om)
     geo = S.SEMQuad(S.Lagrange(N), pm)
-    mod = S.CompressibleIdealGas2D(pm, geo)
+    mod = S.CompressibleIdealGas2D(pm, geo, form=form)
     X, Y = geo_o.x[0, :, :, 0, :], geo_o.x[1, :, :, 0, :]
     q = np.zeros((8, 8, 4, nx * nx), order="F")
     rho = 1 + 0.1 * np.sin(2 * np.pi * X) * np.sin(2 * np.pi * Y)
@@ -197,29 +216,37 @@ def test_c2_full_size_tendency_and_steps():
     q[:, :, 3] = 1.0 / 0.4 + 0.5 * 0.34
     mod.SetSolution(q)
     d = mod.CalculateTendency()
-    # round-off of the metric identities at h = 1/128 (the oracle's residual is the same, bit for bit)
+    # round-off of the metric identities at h = 1/128 (the oracle's residual is the same, bit for bit,
+    # in the reference-rounding form)
     assert float(d.abs().max()) < 1e-6
     torch.cuda.synchronize()
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("model", ["LSW", "SW", "CIG"])
 @pytest.mark.parametrize("N", [3, 7])
-def test_persistent_kernel_matches_per_element_kernel_bitwise(model, N):
+def test_persistent_kernel_matches_per_element_kernel(model, N, form):
     """The persistent bulk-copy kernel and the per-element-group kernel compute
-    the same values: bit-identical states after RK3 steps."""
+    the same values: bit-identical states after RK3 steps in the
+    reference-rounding form, within 1e-12 in the production form (the two
+    kernels group their multiply-adds differently)."""
     import self_b200 as S
     n, dt = 6, 1e-3
     mesh_kind = "periodic" if model == "CIG" else "flipped"
     outs = []
     for persistent in (1, 0):
-        _, mod, _, _ = build_pair(model, mesh_kind, N, seed=5)
+        _, mod, _, _ = build_pair(model, mesh_kind, N, seed=5, form=form)
         S.check(S.lib().selfgpu_model2d_set_launch(mod._h, persistent, 0))
         mod.ForwardStep(n, dt)
         mod.Sync()
         if persistent:
             assert S.lib().selfgpu_model2d_persistent_launch_count(mod._h) == 3 * n
         outs.append(S.to_host(mod.solution).copy())
-    np.testing.assert_array_equal(outs[0], outs[1])
+    if form == S.FP64_REF:
+        np.testing.assert_array_equal(outs[0], outs[1])
+    else:
+        for v in range(outs[1].shape[2]):
+            assert C.rel_err(outs[0][:, :, v], outs[1][:, :, v]) < TOL
 
 
 @pytest.mark.parametrize("model,N", [("CIG", 7), ("SW", 5), ("LSW", 7)])
@@ -312,7 +339,7 @@ def test_fp32_bulk_form_error_vs_fp64_oracle(model, mesh_kind, N, capsys):
     err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
     with capsys.disabled():
         print(f"\nFP32-bulk {model} N={N}: relative L2 error after 40 steps = {err:.3e}")
-    assert err < 1e-5
+    assert err < 1e-6  # the bar for the mixed-precision forms on smooth cases
 
 
 def test_engine_rejects_malformed_side_info():
@@ -366,12 +393,14 @@ def test_checkpoint_pickup_continues_bit_for_bit(tmp_path):
         wrong.Read(name)
 
 
-def test_c1_gravity_wave_release_1000_steps_bit_exact():
+@pytest.mark.parametrize("form", FORMS)
+def test_c1_gravity_wave_release_1000_steps(form):
     """The LinearShallowWater gravity-wave release exactly as configured for
     the reference's CPU-runnable case: 10x10 walls, N = 7 Legendre-Gauss,
     g = H = 1, f = 0, eta0 = 0.01 exp(-r^2 / 0.1^2), u = v = 0, Rusanov flux,
     RK3 with dt = 1e-4 for 1000 steps: the state equals the oracle's bit for
-    bit (and mass stays conserved to round-off)."""
+    bit in the reference-rounding form and within 1e-12 in the production
+    form."""
     import self_b200 as S
     N, dt, steps = 7, 1e-4, 1000
     kw = dict(nx=10, ny=10, bcid=O.BC_NONORMALFLOW, amp=0.0)
@@ -379,7 +408,7 @@ def test_c1_gravity_wave_release_1000_steps_bit_exact():
     mod_o = O.Model(C.MODELS["LSW"], N, om)
     geo_o = O.Geometry(N, om)
     geo = S.SEMQuad(S.Lagrange(N, S.GAUSS, N, S.UNIFORM), pm)
-    mod = S.LinearShallowWater(pm, geo)
+    mod = S.LinearShallowWater(pm, geo, form=form)
     X, Y = geo_o.x[0, :, :, 0, :], geo_o.x[1, :, :, 0, :]
     P = N + 1
     q0 = np.zeros((P, P, 3, X.shape[2]), order="F")
@@ -397,5 +426,9 @@ def test_c1_gravity_wave_release_1000_steps_bit_exact():
     mod.Sync()
     ref = mod_o.get("solution", q0.shape)
     got = S.to_host(mod.solution).reshape(ref.shape, order="F")
-    np.testing.assert_array_equal(got, ref)
+    if form == S.FP64_REF:
+        np.testing.assert_array_equal(got, ref)
+    else:
+        for v in range(3):
+            assert C.rel_err(got[:, :, v], ref[:, :, v]) < TOL, (v, C.rel_err(got[:, :, v], ref[:, :, v]))
     assert np.isfinite(got).all() and np.abs(got[:, :, 2]).max() > 1e-4

@@ -15,11 +15,14 @@ def _small_instances(seed=3):
 
 
 def test_batched_fp64_equals_unbatched_fp64_bitwise():
+    """Batching changes no arithmetic: in the reference-rounding form (the
+    kernels' per-element arithmetic is then independent of the kernel the
+    autotuner picks) every instance of the batch equals its own run."""
     import self_b200 as S
     from self_b200 import ensemble as E
     inst = _small_instances()
-    ens = E.ShallowWaterEnsemble(inst, form=S.FP64, autotune=True)
-    ref = E.UnbatchedShallowWater(inst)
+    ens = E.ShallowWaterEnsemble(inst, form=S.FP64_REF, autotune=True)
+    ref = E.UnbatchedShallowWater(inst, form=S.FP64_REF)
     ens.ForwardStep(15)
     ref.ForwardStep(15)
     torch.cuda.synchronize()

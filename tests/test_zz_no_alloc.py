@@ -3,11 +3,13 @@
 selfgpu_cig2d_tendency_noalloc serves callers that may not allocate device
 memory when they need a tendency (all device memory owned by the host code, a
 hard memory cap, no allocator calls allowed inside a solver step).  Its
-scratch is a fixed device array inside the library.  This test calls it
-through the C ABI twice in a row, on two different states, and checks each
-result against the engine's selfgpu_model2d_tendency on the same inputs, with
-the 1e-12 relative tolerance of the other parity tests.  It also checks that a
-mesh too large for the fixed array is refused with a clear error.
+scratch is a fixed device array inside the library.  These tests call it
+through the C ABI twice in a row, on two different states, and check each
+result against the engine's selfgpu_model2d_tendency on the same inputs: bit
+for bit against the reference-rounding form (SELFGPU_FP64_REF, the same
+arithmetic) and within the 1e-12 relative tolerance of the other parity tests
+against the production FP64 form.  They also check the fixed-size limit at
+N = 3 from both sides and the refusal of boundary conditions it cannot serve.
 
 This file is collected last so that a run stopping at the first failure has
 run every other test before it.
@@ -20,6 +22,7 @@ import torch
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
+SCRATCH_BYTES = 16 * 1024 * 1024  # SELFGPU_NOALLOC_SCRATCH_BYTES
 
 
 def _state(x, seed):
@@ -38,14 +41,13 @@ def _rel(got, ref):
     return float((got - ref).abs().max() / ref.abs().max())
 
 
-def test_noalloc_tendency_matches_engine_on_two_calls_in_a_row():
-    import self_b200 as S
-    N = 7
-    mesh = S.Mesh2D(6, 5, periodic=(True, False), perturbation=0.04, bcid=S.BC_NONORMALFLOW,
-                    rotation=[0, 1, 2, 3, 0] * 6)
-    interp = S.Lagrange(N)
-    geo = S.SEMQuad(interp, mesh)
-    model = S.CompressibleIdealGas2D(mesh, geo)
+def _limit(N):
+    """Largest element count the fixed scratch takes at degree N."""
+    block = (9 * (N + 1) + 1) // 2 * 2  # values per (element, side) trace block
+    return SCRATCH_BYTES // (4 * block * 8)
+
+
+def _call(S, q, out, geo, mesh, interp, gamma):
     L = S.lib()
     dg = np.asfortranarray(interp.dgMatrix)
     bm = np.asfortranarray(interp.bMatrix)
@@ -53,18 +55,68 @@ def test_noalloc_tendency_matches_engine_on_two_calls_in_a_row():
     si_h = np.asfortranarray(mesh.sideInfo)
     host = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
     dev = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    return L.selfgpu_cig2d_tendency_noalloc(dev(q), dev(out), dev(geo.dsdx), dev(geo.J), dev(geo.nHat),
+                                            dev(geo.nScale), dev(mesh.sideInfo_d), host(si_h), host(dg),
+                                            host(bm), host(qw), gamma, interp.N, mesh.nElem, None)
+
+
+def _check_two_calls(S, mesh, N):
+    interp = S.Lagrange(N)
+    geo = S.SEMQuad(interp, mesh)
+    ref_model = S.CompressibleIdealGas2D(mesh, geo, form=S.FP64_REF)
+    prod_model = S.CompressibleIdealGas2D(mesh, geo, form=S.FP64)
     for seed in (1, 2):  # two calls in a row, on different states
         q = _state(geo.x, seed)
-        model.SetSolution(q)
-        ref = model.CalculateTendency().clone()
+        ref_model.SetSolution(q)
+        ref = ref_model.CalculateTendency().clone()
+        prod_model.SetSolution(q)
+        prod = prod_model.CalculateTendency().clone()
         out = torch.full_like(ref, float("nan"))
-        rc = L.selfgpu_cig2d_tendency_noalloc(dev(q), dev(out), dev(geo.dsdx), dev(geo.J), dev(geo.nHat),
-                                              dev(geo.nScale), dev(mesh.sideInfo_d), host(si_h), host(dg),
-                                              host(bm), host(qw), model.expansionFactor, N, mesh.nElem, None)
-        assert rc == 0, L.selfgpu_last_error()
+        rc = _call(S, q, out, geo, mesh, interp, ref_model.expansionFactor)
+        assert rc == 0, S.lib().selfgpu_last_error()
         torch.cuda.synchronize()
         assert torch.isfinite(out).all()
-        assert _rel(out, ref) < TOL
+        assert torch.equal(out, ref)
+        assert _rel(out, prod) < TOL
+
+
+@pytest.mark.parametrize("N", [1, 3, 5, 7])
+def test_noalloc_tendency_matches_engine_on_two_calls_in_a_row(N):
+    import self_b200 as S
+    mesh = S.Mesh2D(6, 5, periodic=(True, False), perturbation=0.04, bcid=S.BC_NONORMALFLOW,
+                    rotation=[0, 1, 2, 3, 0] * 6)
+    _check_two_calls(S, mesh, N)
+
+
+def test_noalloc_at_the_element_limit_at_n3():
+    """The largest mesh the fixed scratch takes at N = 3 (one row of elements,
+    walls all round) runs and matches the engine; one element more is
+    refused."""
+    import self_b200 as S
+    N = 3
+    n = _limit(N)
+    assert n == 14563
+    _check_two_calls(S, S.Mesh2D(n, 1, bcid=S.BC_NONORMALFLOW), N)
+    big = S.Mesh2D(n + 1, 1, bcid=S.BC_NONORMALFLOW)
+    interp = S.Lagrange(N)
+    geo = S.SEMQuad(interp, big)
+    q = torch.zeros((big.nElem, 4, N + 1, N + 1), device="cuda", dtype=torch.float64)
+    rc = _call(S, q, q.clone(), geo, big, interp, 1.4)
+    assert rc == 1
+    assert b"fixed limit" in S.lib().selfgpu_last_error()
+
+
+def test_noalloc_rejects_boundary_conditions_it_cannot_serve():
+    import self_b200 as S
+    N = 3
+    for bc in (S.BC_PRESCRIBED, S.BC_RADIATION):
+        mesh = S.Mesh2D(3, 3, bcid=bc)
+        interp = S.Lagrange(N)
+        geo = S.SEMQuad(interp, mesh)
+        q = torch.ones((mesh.nElem, 4, N + 1, N + 1), device="cuda", dtype=torch.float64)
+        rc = _call(S, q, q.clone(), geo, mesh, interp, 1.4)
+        assert rc == 1
+        assert b"NONORMALFLOW" in S.lib().selfgpu_last_error()
 
 
 def test_noalloc_rejects_meshes_beyond_its_fixed_scratch():
@@ -74,7 +126,7 @@ def test_noalloc_rejects_meshes_beyond_its_fixed_scratch():
     si = np.zeros(20, dtype=np.int32)
     d = ctypes.c_void_p(buf.data_ptr())
     h = si.ctypes.data_as(ctypes.c_void_p)
-    too_many = 8000  # 8000 elements at N = 7 need 18.4 MB of face-trace scratch
+    too_many = _limit(7) + 1  # 7282 elements at N = 7 need more than the 16 MiB of face-trace scratch
     rc = L.selfgpu_cig2d_tendency_noalloc(d, d, d, d, d, d, d, h, h, h, h, 1.4, 7, too_many, None)
     assert rc == 1
     assert b"fixed limit" in L.selfgpu_last_error()
