@@ -372,29 +372,6 @@ def _rel_l2(a, b):
     return d if np.isfinite(d) else None
 
 
-def shock_band(x, rng):
-    """Smooth density wave (the C2 state) plus one seeded shock-tube band: in
-    |y - y0| < 0.05 a Sod-like tube (rho, p) = (1, 1) | (0.125, 0.1) at rest,
-    split at x = x0."""
-    import torch
-    X, Y = x[:, 0, :, :, 0], x[:, 0, :, :, 1]
-    x0, y0 = rng.uniform(0.3, 0.7, size=2)
-    rho = 1.0 + 0.1 * torch.sin(2 * np.pi * X) * torch.sin(2 * np.pi * Y)
-    u = torch.full_like(X, 0.5)
-    v = torch.full_like(X, 0.3)
-    p = torch.ones_like(X)
-    band = (Y - y0).abs() < 0.05
-    left = X < x0
-    rho = torch.where(band, torch.where(left, torch.ones_like(X), torch.full_like(X, 0.125)), rho)
-    p = torch.where(band, torch.where(left, torch.ones_like(X), torch.full_like(X, 0.1)), p)
-    u = torch.where(band, torch.zeros_like(X), u)
-    v = torch.where(band, torch.zeros_like(X), v)
-    q = torch.empty((X.shape[0], 4) + tuple(X.shape[1:]), device=X.device, dtype=torch.float64)
-    q[:, 0], q[:, 1], q[:, 2] = rho * u, rho * v, rho
-    q[:, 3] = p / (GAMMA - 1.0) + 0.5 * rho * (u * u + v * v)
-    return q
-
-
 def _closure_variant(mesh, geo, q0, form, mode, mlp, steps, dt, dof, nvtx=None):
     """One timed run from q0: DOF-updates/s, the final state and closure statistics
     (the timed steps inside an NVTX range named nvtx, for profilers)."""
@@ -504,7 +481,7 @@ def measure_c5(mlp7, steps=100):
     interp = S.Lagrange(7, S.GAUSS, 7, S.UNIFORM)
     mesh = S.Mesh2D(512, 512, periodic=(True, True), perturbation=0.02)
     geo = S.SEMQuad(interp, mesh)
-    q0 = shock_band(geo.x, np.random.Generator(np.random.PCG64(200)))
+    q0 = CL.shock_band(geo.x, np.random.Generator(np.random.PCG64(200)), gamma=GAMMA)
     dt = CL.stable_dt(S.CompressibleIdealGas2D(mesh, geo), q0)
     return _closure_workload("c5", mesh, geo, q0, dt, 4 * 64 * mesh.nElem, steps, mlp7,
                              f"CIG periodic 512x512 perturbed N=7, smooth density wave + shock-tube band, {steps} RK3 "
@@ -559,12 +536,69 @@ def measure_c1():
             "value": 19200 * 1000 / (ms / 1e3), "unit": "DOF-updates/s", "ms_per_rk3_step": ms / 1000}
 
 
+def measure_gas_ensemble(mlps, steps=100, n_instances=256):
+    """The batched FP32-bulk + learned-closure form on an ensemble of uneven
+    CompressibleIdealGas2D instances (nx, ny ~ U{8..64}, N ~ U{5, 7}, periodic,
+    perturbed, smooth density waves, a seeded quarter with a shock-tube band),
+    against the plain FP64 GPU form on the same instances (one handle per
+    instance, and batched), with the FP64 indicator-closure run as the judge on
+    shocked members.  Rates over `steps` RK3 steps; errors after them."""
+    import torch
+
+    import self_b200 as S
+    from self_b200 import ensemble as E
+    inst = E.make_gas_instances(n_instances, seed=0)
+    variants = [("batched_fp32_learned", dict(form=S.FP32_BULK, closure=S.CLOSURE_MLP, mlps=mlps)),
+                ("batched_fp32_indicator", dict(form=S.FP32_BULK, closure=S.CLOSURE_INDICATOR)),
+                ("batched_fp64_indicator", dict(form=S.FP64, closure=S.CLOSURE_INDICATOR)),
+                ("batched_fp64_plain", dict(form=S.FP64))]
+    runners = {name: E.CompressibleGasEnsemble(inst, autotune=True, **kw) for name, kw in variants}
+    runners["unbatched_fp64_plain"] = E.UnbatchedGas(inst)
+    dof = sum(i.dof() for i in inst)
+    n_smooth = sum(1 for i in inst if i.smooth)
+    out = {"workload": f"{n_instances} CompressibleIdealGas2D instances, nx,ny~U{{8..64}}, N~U{{5,7}}, periodic "
+                       f"perturbed 0.02h, smooth density waves ({n_smooth} smooth, {n_instances - n_smooth} with a "
+                       f"shock-tube band), per-instance CFL/viscous step; rates over {steps} RK3 steps",
+           "dof": dof}
+    for name, r in runners.items():
+        r.reset()
+        r.ForwardStep(2)
+        torch.cuda.synchronize()
+        r.reset()
+        t = E.time_it(lambda: r.ForwardStep(steps))
+        out[name] = {"value": dof * steps / t, "unit": "DOF-updates/s", "ms_per_rk3_step": 1e3 * t / steps}
+        if hasattr(r, "tuning"):
+            out[name]["autotune"] = {f"N={k}": v for k, v in r.tuning.items()}
+    lead = out["batched_fp32_learned"]["value"]
+    out["speedup_fp32_learned_batched_vs_unbatched_fp64_plain"] = lead / out["unbatched_fp64_plain"]["value"]
+    out["speedup_fp32_learned_batched_vs_batched_fp64_plain"] = lead / out["batched_fp64_plain"]["value"]
+    # errors after `steps`: smooth members against the plain FP64 run, shocked
+    # members against the FP64 indicator-closure run
+    worst_smooth, worst_shock = 0.0, 0.0
+    L, P64, I64 = runners["batched_fp32_learned"], runners["batched_fp64_plain"], runners["batched_fp64_indicator"]
+    for it in inst:
+        a = L.solution(it)
+        b = (P64 if it.smooth else I64).solution(it)
+        e = float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+        if it.smooth:
+            worst_smooth = max(worst_smooth, e)
+        else:
+            worst_shock = max(worst_shock, e)
+    out[f"fp32_learned_worst_rel_l2_vs_fp64_plain_smooth_members_after_{steps}_steps"] = worst_smooth
+    out[f"fp32_learned_worst_rel_l2_vs_fp64_indicator_shocked_members_after_{steps}_steps"] = worst_shock
+    out["all_finite"] = bool(all(torch.isfinite(L.solution(it)).all() for it in inst))
+    del runners
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_closure_forms():
     """The learned shock closure (form 4), the large single solve with all
-    forms, C2 in the FP32-bulk form and C1."""
+    forms, the batched learned-closure ensemble, C2 in the FP32-bulk form and C1."""
     out, mlps = train_closures()
     out["c4_learned_closure"] = measure_c4(mlps[5])
     out["c5_large_solve"] = measure_c5(mlps[7])
+    out["gas_ensemble_fp32_learned"] = measure_gas_ensemble(mlps)
     out["c2_forms"] = measure_c2_forms()
     out["c1_lsw"] = measure_c1()
     return out
@@ -573,6 +607,10 @@ def run_closure_forms():
 def run_one_form(name):
     if name == "ensemble":
         return run_forms()
+    if name == "gas_ensemble":
+        out, mlps = train_closures()
+        out["gas_ensemble_fp32_learned"] = measure_gas_ensemble(mlps)
+        return out
     if name == "c1":
         return measure_c1()
     if name == "c2":
@@ -780,7 +818,7 @@ def main():
     ap.add_argument("--impl", default="selfgpu", choices=["selfgpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the ensemble / FP32-bulk form measurements")
-    ap.add_argument("--form", choices=["c1", "c2", "c4", "c5", "ensemble"], default=None,
+    ap.add_argument("--form", choices=["c1", "c2", "c4", "c5", "ensemble", "gas_ensemble"], default=None,
                     help="run only this form's measurement and print its JSON (diagnostic mode)")
     ap.add_argument("--cpu-table", action="store_true",
                     help="print the CPU-baseline table of configs C1-C5 (oracle port) and exit")

@@ -267,7 +267,8 @@ int selfgpu_model2d_set_state(selfgpu_model2d* m, double* solution, double* work
 
 /* Model-specific device fields (caller owned), by name:
  *  LSW: "H" interior (P,P,1,nEl), "H.boundary" (P,1,4,nEl), "fCori" interior
- *  SW : "topography.boundary" (P,1,4,nEl), "gradTopography" (2,P,P,1,nEl)
+ *  SW : "topography.boundary" (P,1,4,nEl), "gradTopography" (2,P,P,1,nEl),
+ *       "topography" (P,P,1,nEl; read by selfgpu_model2d_entropy only)
  *  CIG: "environmentalsGradient" (2,P,P,2,nEl), "environmentals" (P,P,2,nEl),
  *       "prescribedSolution.boundary", "prescribedPrimitive.boundary",
  *       "prescribedDiagnostics.boundary" (P,4,4,nEl each)
@@ -296,6 +297,15 @@ int selfgpu_model2d_rk3(selfgpu_model2d* m, double dt, int nSteps);
 
 /* Wait for the engine's stream; returns the first pending CUDA error. */
 int selfgpu_model2d_sync(selfgpu_model2d* m);
+
+/* CalculateEntropy of the bound model on the device, returned on the host
+ * (the stream is synchronised): LSW src/models/SELF_LinearShallowWater.f90:171-216,
+ * SW src/models/SELF_ShallowWater.f90:149-188 (reads the interior field
+ * "topography"), CIG src/models/SELF_CompressibleIdealGas2D.f90:782-823 (p
+ * formed from the current solution; the reference reads the primitive field
+ * of its last PreTendency).  Per-element sums in the reference's node order,
+ * then a fixed-order tree over the elements. */
+int selfgpu_model2d_entropy(selfgpu_model2d* m, double* entropy);
 
 /* Scan the solution for NaN/Inf on the device (SELFGPU_ERR_NONFINITE if any). */
 int selfgpu_model2d_check_finite(selfgpu_model2d* m);

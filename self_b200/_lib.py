@@ -40,6 +40,7 @@ _SIGS = {
     "selfgpu_model2d_rk3": (c_int, [c_void_p, c_double, c_int]),
     "selfgpu_model2d_sync": (c_int, [c_void_p]),
     "selfgpu_model2d_check_finite": (c_int, [c_void_p]),
+    "selfgpu_model2d_entropy": (c_int, [c_void_p, ctypes.POINTER(c_double)]),
     "selfgpu_model2d_launch_count": (c_longlong, [c_void_p]),
     "selfgpu_model2d_persistent_launch_count": (c_longlong, [c_void_p]),
     "selfgpu_model2d_set_kernel": (c_int, [c_void_p, c_int]),

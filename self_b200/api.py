@@ -259,6 +259,14 @@ class Model2D:
     def CheckFinite(self):
         check(lib().selfgpu_model2d_check_finite(self._h))
 
+    def CalculateEntropy(self):
+        """CalculateEntropy of the model (src/models/SELF_*.f90), reduced on the
+        device; kept in self.entropy as the reference keeps it."""
+        e = ctypes.c_double()
+        check(lib().selfgpu_model2d_entropy(self._h, ctypes.byref(e)))
+        self.entropy = e.value
+        return self.entropy
+
     def LaunchCount(self):
         return lib().selfgpu_model2d_launch_count(self._h)
 
@@ -286,10 +294,6 @@ class LinearShallowWater(Model2D):
         fi = (f if isinstance(f, torch.Tensor) else to_device(f)).reshape(nEl, 1, P, P).contiguous()
         self._set_field("fCori", fi)
 
-    def CalculateEntropy(self):
-        u, v, eta = self.solution[:, 0], self.solution[:, 1], self.solution[:, 2]
-        H = self._fields["H"][:, 0]
-        return float((0.5 * (H * (u * u + v * v) + self.g * eta * eta) * self._wJ()).sum())
 
 
 class ShallowWater(Model2D):
@@ -304,14 +308,10 @@ class ShallowWater(Model2D):
         P, nEl = self.N + 1, self.nElem
         hi = (h if isinstance(h, torch.Tensor) else to_device(h)).reshape(nEl, 1, P, P).contiguous()
         self.topography = hi
+        self._set_field("topography", hi)
         self._set_field("topography.boundary", self._bnd_interp(hi, 1))
         self._set_field("gradTopography", self._gradient_sf(hi, 1))
 
-    def CalculateEntropy(self):
-        Hu, Hv, H = self.solution[:, 0], self.solution[:, 1], self.solution[:, 2]
-        b = self.topography[:, 0]
-        e = 0.5 * (Hu * Hu / H + Hv * Hv / H) + 0.5 * self.g * H * H - self.g * H * b
-        return float((e * self._wJ()).sum())
 
 
 class CompressibleIdealGas2D(Model2D):
@@ -402,8 +402,3 @@ class CompressibleIdealGas2D(Model2D):
                                                   int(reset)))
         return nu, act, ind, (counts[0], counts[1])
 
-    def CalculateEntropy(self):
-        prim = self._pointwise("primitive")
-        rho, p = self.solution[:, 2], prim[:, 3]
-        g = self.expansionFactor
-        return float((rho * (torch.log(p) - g * torch.log(rho)) / (g - 1.0) * self._wJ()).sum())

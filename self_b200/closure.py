@@ -156,6 +156,29 @@ def riemann_quadrants(x, rng, gamma=1.4, rho=(0.1, 1.5), p=(0.1, 1.5), umax=1.0,
     return q
 
 
+def shock_band(x, rng, gamma=1.4):
+    """Smooth density wave (rho = 1 + 0.1 sin(2 pi x) sin(2 pi y), (u, v) =
+    (0.5, 0.3), p = 1) plus one seeded shock-tube band: in |y - y0| < 0.05 a
+    Sod-like tube (rho, p) = (1, 1) | (0.125, 0.1) at rest, split at x = x0.
+    x: node coordinates (nEl, 1, P, P, 2); returns (nEl, 4, P, P) conservative."""
+    X, Y = x[:, 0, :, :, 0], x[:, 0, :, :, 1]
+    x0, y0 = rng.uniform(0.3, 0.7, size=2)
+    rho = 1.0 + 0.1 * torch.sin(2 * np.pi * X) * torch.sin(2 * np.pi * Y)
+    u = torch.full_like(X, 0.5)
+    v = torch.full_like(X, 0.3)
+    p = torch.ones_like(X)
+    band = (Y - y0).abs() < 0.05
+    left = X < x0
+    rho = torch.where(band, torch.where(left, torch.ones_like(X), torch.full_like(X, 0.125)), rho)
+    p = torch.where(band, torch.where(left, torch.ones_like(X), torch.full_like(X, 0.1)), p)
+    u = torch.where(band, torch.zeros_like(X), u)
+    v = torch.where(band, torch.zeros_like(X), v)
+    q = torch.empty((X.shape[0], 4) + tuple(X.shape[1:]), device=X.device, dtype=torch.float64)
+    q[:, 0], q[:, 1], q[:, 2] = rho * u, rho * v, rho
+    q[:, 3] = p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v)
+    return q
+
+
 def stable_dt(model, q, c_av=1.0, cfl=0.5, cfl_visc=0.25, gamma=1.4):
     """Time step for the closure run: min of the advective CFL step and the
     explicit viscous limit with the largest viscosity the closure can give."""

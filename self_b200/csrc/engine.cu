@@ -77,6 +77,58 @@ __global__ void k_move_blocks(const uint32_t* __restrict__ src, const int* __res
   }
 }
 
+// Entropy integrands (CalculateEntropy of the three models), summed per
+// element in the reference's node order (j outer, i inner):
+//   LSW  0.5 (H (u^2 + v^2) + g eta^2) J w_i w_j  (src/models/SELF_LinearShallowWater.f90:171-216)
+//   SW   (0.5 (Hu^2/H + Hv^2/H) + 0.5 g H^2 - g H b) J w_i w_j  (src/models/SELF_ShallowWater.f90:149-188)
+//   CIG  rho (log p - gamma log rho) / (gamma - 1) w_i w_j J, p from the
+//        solution as ConservativeToPrimitive forms it (src/models/SELF_CompressibleIdealGas2D.f90:782-823)
+// `aux` is H (LSW) or the topography b (SW), (P,P,1,nEl).
+__global__ void k_entropy_elements(int model, const double* __restrict__ q, const double* __restrict__ J,
+                                   const double* __restrict__ aux, QwArr qw, int P, int nEl, double g, double gamma,
+                                   double* __restrict__ out) {
+  const int PP = P * P;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nEl; e += (long long)gridDim.x * blockDim.x) {
+    const int nv = model == SELFGPU_MODEL_CIG ? 4 : 3;
+    const double* qe = q + (size_t)nv * PP * e;
+    double s = 0.0;
+    for (int j = 0; j < P; ++j)
+      for (int i = 0; i < P; ++i) {
+        const int n = i + P * j;
+        const double Jac = J[n + (size_t)PP * e], wi = qw.w[i], wj = qw.w[j];
+        if (model == SELFGPU_MODEL_LSW) {
+          const double u = qe[n], v = qe[n + PP], eta = qe[n + 2 * PP], H = aux[n + (size_t)PP * e];
+          s = s + 0.5 * (H * (u * u + v * v) + g * eta * eta) * Jac * wi * wj;
+        } else if (model == SELFGPU_MODEL_SW) {
+          const double Hu = qe[n], Hv = qe[n + PP], H = qe[n + 2 * PP];
+          const double b = aux ? aux[n + (size_t)PP * e] : 0.0;
+          s = s + (0.5 * (Hu * Hu / H + Hv * Hv / H) + 0.5 * g * H * H - g * H * b) * Jac * wi * wj;
+        } else {
+          const double rhoU = qe[n], rhoV = qe[n + PP], rho = qe[n + 2 * PP], rhoE = qe[n + 3 * PP];
+          const double u = rhoU / rho, v = rhoV / rho;
+          const double p = (gamma - 1.0) * (rhoE - 0.5 * (rhoU * u + rhoV * v));
+          s = s + rho * (log(p) - gamma * log(rho)) / (gamma - 1.0) * wi * wj * Jac;
+        }
+      }
+    out[e] = s;
+  }
+}
+
+// Deterministic sum of n values by one block: strided partial sums, then a
+// shared-memory tree.  The result lands in out[0].
+__global__ void __launch_bounds__(1024) k_sum_block(const double* __restrict__ x, long long n, double* out) {
+  __shared__ double part[1024];
+  double s = 0.0;
+  for (long long k = threadIdx.x; k < n; k += blockDim.x) s += x[k];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = part[0];
+}
+
 int nt_of(int model) { return model == SELFGPU_MODEL_CIG ? 9 : 3; }
 int nv_of(int model) { return model == SELFGPU_MODEL_CIG ? 4 : 3; }
 
@@ -116,6 +168,7 @@ struct selfgpu_model2d {
   __nv_bfloat16* mlpW = nullptr;
   float* mlpB = nullptr;
   double* geo = nullptr;  // packed geometry records (persistent kernel)
+  double* entropyBuf = nullptr;  // per-element entropy sums (nEl) and the total
 
   size_t elemBytes() const { return form == SELFGPU_FP32_BULK ? sizeof(float) : sizeof(double); }
 
@@ -302,7 +355,7 @@ int selfgpu_model2d_destroy(selfgpu_model2d* m) {
     if (m->vel[k]) cudaFree(m->vel[k]);
   }
   for (void* p : {(void*)m->avNu, (void*)m->avAct, (void*)m->avFallbacks, (void*)m->avH, m->avVisc, m->avVtr,
-                  (void*)m->mlpW, (void*)m->mlpB, (void*)m->geo})
+                  (void*)m->mlpW, (void*)m->mlpB, (void*)m->geo, (void*)m->entropyBuf})
     if (p) cudaFree(p);
   if (m->dflag) cudaFree(m->dflag);
   if (m->ownStream) cudaStreamDestroy(m->stream);
@@ -386,6 +439,7 @@ int selfgpu_model2d_set_field(selfgpu_model2d* m, const char* name, const double
   } else if (m->model == SELFGPU_MODEL_SW) {
     if (n == "topography.boundary") slot = 0;
     else if (n == "gradTopography") slot = 1;
+    else if (n == "topography") slot = 2;  // interior topography: read by the entropy only
   } else {
     if (n == "environmentalsGradient") slot = 0;
     else if (n == "environmentals") slot = 1;
@@ -851,6 +905,32 @@ int selfgpu_model2d_check_finite(selfgpu_model2d* m) {
   cudaError_t e = cudaStreamSynchronize(m->stream);
   if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_check_finite", e);
   if (h) return set_error(SELFGPU_ERR_NONFINITE, "selfgpu_model2d_check_finite: solution holds NaN or Inf");
+  return SELFGPU_OK;
+}
+
+int selfgpu_model2d_entropy(selfgpu_model2d* m, double* entropy) {
+  int rc = check_ready(m, "selfgpu_model2d_entropy");
+  if (rc) return rc;
+  if (!entropy) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_entropy: null output");
+  const double* aux = nullptr;
+  if (m->model == SELFGPU_MODEL_LSW) aux = m->base.fld[0];
+  else if (m->model == SELFGPU_MODEL_SW) aux = m->base.fld[2];
+  if (!m->haveInterp) return set_error(SELFGPU_ERR_STATE, "selfgpu_model2d_entropy: no interpolant");
+  cudaError_t e = cudaSuccess;
+  if (!m->entropyBuf) e = cudaMalloc(&m->entropyBuf, ((size_t)m->nEl + 1) * sizeof(double));
+  if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_entropy", e);
+  QwArr w{};
+  for (int k = 0; k < m->P; ++k) w.w[k] = m->base.qw[k];
+  const int blocks = (m->nEl + 127) / 128 < 1184 ? (m->nEl + 127) / 128 : 1184;
+  k_entropy_elements<<<blocks, 128, 0, m->stream>>>(m->model, m->base.q, m->base.J, aux, w, m->P, m->nEl, m->base.g,
+                                                    m->base.gamma, m->entropyBuf);
+  k_sum_block<<<1, 1024, 0, m->stream>>>(m->entropyBuf, m->nEl, m->entropyBuf + m->nEl);
+  m->launches += 2;
+  double h = 0.0;
+  e = cudaMemcpyAsync(&h, m->entropyBuf + m->nEl, sizeof(double), cudaMemcpyDeviceToHost, m->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+  if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_entropy", e);
+  *entropy = h;
   return SELFGPU_OK;
 }
 

@@ -31,6 +31,9 @@
 namespace {
 
 int hip_status(cudaError_t e) {
+  // a failed call leaves its code as the runtime's last error; clear it so
+  // that a later, unrelated cudaGetLastError() does not report it again
+  if (e != cudaSuccess) cudaGetLastError();
   switch (e) {
     case cudaSuccess: return 0;
     case cudaErrorInvalidValue: return 1;

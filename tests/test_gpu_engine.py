@@ -20,6 +20,52 @@ TOL = 1e-12
 FORMS = [0, 2]  # self_b200.FP64 (production), self_b200.FP64_REF (reference roundings)
 
 
+def build_oracle(model, mesh_kind, N, seed=0, fast=False):
+    """The oracle half of build_pair; fast=True builds it from the oracle's
+    multiply-add-contracted build (a second valid FP64 rounding of the same
+    reference loops)."""
+    kw = C.mesh_kwargs(mesh_kind)
+    om = C.oracle_mesh(kw)
+    mod_o = O.Model(C.MODELS[model], N, om, fast=fast)
+    x = O.Geometry(N, om).x
+    aux = C.aux_fields(model, x, seed)
+    if model == "LSW":
+        mod_o.set("H", aux["H"])
+        mod_o.set("fCori", aux["fCori"])
+    elif model == "SW":
+        mod_o.set("topography", aux["topography"])
+    else:
+        mod_o.set("gravityPotential", aux["gravityPotential"])
+        mod_o.set("drag", aux["drag"])
+    mod_o.set("solution", C.initial_state(model, x, seed))
+    if model == "CIG" and kw.get("bcid") in (O.BC_PRESCRIBED, O.BC_RADIATION):
+        mod_o.set("prescribed")
+    return mod_o
+
+
+def check_tendency(got, ref, form, model, mesh_kind, N, seed):
+    """Tendency parity.  Reference-rounding form: 1e-12 relative per field
+    (max |difference| / max |oracle value|; it is bit-exact in practice).
+    Production form: per field, within 1e-12 relative or within 8x the
+    oracle's own sensitivity to rounding order on the same inputs (its
+    contracted build against its plain build), whichever is larger.  Where a
+    field's tendency is a small difference of large weak-form terms (the
+    ShallowWater thickness on periodic meshes, the density at 128 x 128), any
+    change of rounding order moves it by more than 1e-12 of its own size, the
+    reference's too."""
+    import self_b200 as S
+    if form == S.FP64_REF:
+        for v in range(ref.shape[2]):
+            assert C.rel_err(got[:, :, v], ref[:, :, v]) < TOL, (v, C.rel_err(got[:, :, v], ref[:, :, v]))
+        return
+    alt = build_oracle(model, mesh_kind, N, seed, fast=True).tendency()
+    for v in range(ref.shape[2]):
+        scale = np.abs(ref[:, :, v]).max()
+        sens = np.abs(alt[:, :, v] - ref[:, :, v]).max()
+        diff = np.abs(got[:, :, v] - ref[:, :, v]).max()
+        assert diff <= max(TOL * scale, 8.0 * sens), (v, diff / scale, sens / scale)
+
+
 def build_pair(model, mesh_kind, N, seed=0, form=0):
     import self_b200 as S
     kw = C.mesh_kwargs(mesh_kind)
@@ -78,8 +124,7 @@ def test_tendency_matches_oracle(model, mesh_kind, N, form):
     mod_o, mod, _, _ = build_pair(model, mesh_kind, N, form=form)
     ref = mod_o.tendency()
     got = S.to_host(mod.CalculateTendency()).reshape(ref.shape, order="F")
-    for v in range(ref.shape[2]):
-        assert C.rel_err(got[:, :, v], ref[:, :, v]) < TOL, (v, C.rel_err(got[:, :, v], ref[:, :, v]))
+    check_tendency(got, ref, form, model, mesh_kind, N, 0)
     # a second call with the same solution gives the same tendency (trace cache reuse)
     got2 = S.to_host(mod.CalculateTendency()).reshape(ref.shape, order="F")
     if model != "SW":  # SW's velocity traces lag one call behind the solution traces by design
@@ -164,7 +209,10 @@ def test_edge_meshes(model, mesh_kind, N, form):
     ref = mod_o.tendency()
     got = S.to_host(mod.CalculateTendency()).reshape(ref.shape, order="F")
     assert np.isfinite(ref).all()
-    same(got, ref)
+    if form == S.FP64_REF:
+        same(got, ref)
+    else:
+        check_tendency(got, ref, form, model, mesh_kind, N, 5)
     mod_o2, mod2, _, _ = build_pair(model, mesh_kind, N, seed=5, form=form)
     mod_o2.rk3(5, 1e-3)
     mod2.ForwardStep(5, 1e-3)
@@ -197,8 +245,18 @@ def test_c2_full_size_tendency_and_steps(form):
     mod.SetSolution(q)
     ref = mod_o.tendency()
     got = S.to_host(mod.CalculateTendency()).reshape(ref.shape, order="F")
-    for v in range(4):
-        assert C.rel_err(got[:, :, v], ref[:, :, v]) < TOL
+    if form == S.FP64_REF:
+        for v in range(4):
+            assert C.rel_err(got[:, :, v], ref[:, :, v]) < TOL
+    else:  # the bound of check_tendency: 1e-12 or 8x the oracle's own rounding sensitivity
+        alt_o = O.Model(O.CIG, N, om, fast=True)
+        alt_o.set("solution", q)
+        alt = alt_o.tendency()
+        for v in range(4):
+            scale = np.abs(ref[:, :, v]).max()
+            sens = np.abs(alt[:, :, v] - ref[:, :, v]).max()
+            diff = np.abs(got[:, :, v] - ref[:, :, v]).max()
+            assert diff <= max(TOL * scale, 8.0 * sens), (v, diff / scale, sens / scale)
     # discrete conservation: sum of J w_i w_j dSdt vanishes on a periodic mesh
     w = S.Lagrange(N).qWeights
     wJ = geo_o.J[:, :, 0, :] * w[:, None, None] * w[None, :, None]
@@ -362,16 +420,20 @@ def test_check_finite_flags_injected_nan():
     assert ei.value.code == 5
 
 
-def test_checkpoint_pickup_continues_bit_for_bit(tmp_path):
+@pytest.mark.parametrize("form", FORMS)
+def test_checkpoint_pickup_continues(tmp_path, form):
     """Write_Model2D after some steps, Read_Model2D into a fresh model: the
-    continued run equals the uninterrupted one bit for bit (the first RK3 stage
-    multiplies the RK register by a_1 = 0, so the solution is the whole
-    state), and the file carries the reference's dataset paths and shapes."""
+    continued run equals the uninterrupted one (the first RK3 stage multiplies
+    the RK register by a_1 = 0, so the solution is the whole state) bit for
+    bit in the reference-rounding form; in the production form within 1e-12
+    (a pickup rebuilds the face-trace cache with the per-element kernel, whose
+    multiply-adds the compiler may group differently from the persistent
+    kernel's), and the file carries the reference's dataset paths and shapes."""
     import self_b200 as S
     from self_b200.checkpoint import Checkpoint
     N, dt = 5, 1e-3
-    _, a, _, _ = build_pair("CIG", "periodic", N, seed=9)
-    _, b, _, _ = build_pair("CIG", "periodic", N, seed=9)
+    _, a, _, _ = build_pair("CIG", "periodic", N, seed=9, form=form)
+    _, b, _, _ = build_pair("CIG", "periodic", N, seed=9, form=form)
     a.ForwardStep(6, dt)
     name = a.Write(str(tmp_path / "pick.ckpt"))
     with Checkpoint(name) as c:
@@ -387,7 +449,10 @@ def test_checkpoint_pickup_continues_bit_for_bit(tmp_path):
     b.Read(name)
     assert b.t == pytest.approx(6 * dt)
     b.ForwardStep(5, dt)
-    np.testing.assert_array_equal(S.to_host(b.solution), S.to_host(a.solution))
+    if form == S.FP64_REF:
+        np.testing.assert_array_equal(S.to_host(b.solution), S.to_host(a.solution))
+    else:
+        assert C.rel_err(S.to_host(b.solution), S.to_host(a.solution)) < TOL
     _, wrong, _, _ = build_pair("CIG", "periodic", 3, seed=9)
     with pytest.raises(S.SelfGpuError):
         wrong.Read(name)
@@ -432,3 +497,22 @@ def test_c1_gravity_wave_release_1000_steps(form):
         for v in range(3):
             assert C.rel_err(got[:, :, v], ref[:, :, v]) < TOL, (v, C.rel_err(got[:, :, v], ref[:, :, v]))
     assert np.isfinite(got).all() and np.abs(got[:, :, 2]).max() > 1e-4
+
+
+@pytest.mark.parametrize("model,mesh_kind", [("LSW", "walls"), ("SW", "flipped"), ("CIG", "periodic"),
+                                             ("CIG", "prescribed")])
+def test_entropy_matches_oracle(model, mesh_kind):
+    """CalculateEntropy reduced on the device against the oracle's
+    restatement of the reference loops, before and after RK3 steps (the
+    oracle's CompressibleIdealGas2D entropy reads the primitive field of its
+    last tendency, so a tendency call refreshes it first)."""
+    N, n, dt = 5, 6, 1e-3
+    mod_o, mod, _, _ = build_pair(model, mesh_kind, N, seed=4)
+    for k in range(2):
+        if k:
+            mod_o.rk3(n, dt)
+            mod.ForwardStep(n, dt)
+        mod_o.tendency()
+        e_o = mod_o.entropy()
+        e = mod.CalculateEntropy()
+        assert e_o != 0.0 and abs(e - e_o) <= 1e-12 * abs(e_o), (k, e, e_o)

@@ -74,3 +74,78 @@ def test_fp32_bulk_ensemble_error_vs_fp64(capsys):
         print(f"\nFP32-bulk ensemble: worst relative L2 error vs FP64 after {n} steps = {worst:.3e}; "
               f"autotune {e32.tuning}")
     assert worst < 1e-6
+
+
+def _gas_instances(seed=4):
+    from self_b200 import ensemble as E
+    inst = E.make_gas_instances(n=6, seed=seed, nmin=3, nmax=6, degrees=(5, 7), shock_fraction=0.5)
+    assert any(i.smooth for i in inst) and any(not i.smooth for i in inst)
+    return inst
+
+
+def test_gas_ensemble_batched_equals_unbatched_bitwise():
+    """CompressibleIdealGas2D instances concatenated per degree advance exactly
+    as they do one handle per instance (reference-rounding FP64, no closure)."""
+    import self_b200 as S
+    from self_b200 import ensemble as E
+    inst = _gas_instances()
+    ens = E.CompressibleGasEnsemble(inst, form=S.FP64_REF, autotune=True)
+    ref = E.UnbatchedGas(inst, form=S.FP64_REF)
+    ens.ForwardStep(6)
+    ref.ForwardStep(6)
+    torch.cuda.synchronize()
+    for it, model, _ in ref.runs:
+        got = ens.solution(it).cpu().numpy()
+        assert np.isfinite(got).all()
+        np.testing.assert_array_equal(got, model.solution.cpu().numpy())
+
+
+def test_gas_ensemble_closure_instance_matches_oracle():
+    """A batched instance with the indicator closure (the closure kernels run
+    over the concatenated element set) equals the oracle's single-instance
+    closure run with the same time step, 1e-12 relative."""
+    import self_b200 as S
+    from self_b200 import ensemble as E
+    from tests import cases as C
+    inst = _gas_instances(seed=6)
+    ens = E.CompressibleGasEnsemble(inst, form=S.FP64, closure=S.CLOSURE_INDICATOR, autotune=False)
+    n = 8
+    ens.ForwardStep(n)
+    torch.cuda.synchronize()
+    for it in inst[:4]:
+        om = O.Mesh(it.nx, it.ny, periodic=(True, True), amp=0.02)
+        mod = O.Model(O.CIG, it.N, om)
+        q0 = ens.handles[it.N]["q0"][it.offset:it.offset + it.nElem]  # the instance's initial state
+        mod.set("solution", np.asfortranarray(S.to_host(q0)))
+        mod.set_closure(1, c=1.0)
+        mod.rk3(n, it.dt)
+        ref = mod.get("solution", (it.N + 1, it.N + 1, 4, it.nElem))
+        got = S.to_host(ens.solution(it)).reshape(ref.shape, order="F")
+        for v in range(4):
+            assert C.rel_err(got[:, :, v], ref[:, :, v]) < 1e-12, (it, v, C.rel_err(got[:, :, v], ref[:, :, v]))
+
+
+def test_gas_ensemble_fp32_learned_error_on_smooth_members(capsys):
+    """The batched FP32-bulk + learned-closure form: on smooth members the
+    relative L2 error against the plain FP64 run stays within 1e-6."""
+    import self_b200 as S
+    from self_b200 import closure as CL
+    from self_b200 import ensemble as E
+    inst = E.make_gas_instances(n=10, seed=12, nmin=6, nmax=12, degrees=(5, 7), shock_fraction=0.3)
+    mlps = {5: CL.ClosureMLP(seed=5), 7: CL.ClosureMLP(seed=7)}
+    e64 = E.CompressibleGasEnsemble(inst, form=S.FP64, autotune=False)
+    e32 = E.CompressibleGasEnsemble(inst, form=S.FP32_BULK, closure=S.CLOSURE_MLP, mlps=mlps, autotune=True)
+    n = 50
+    e64.ForwardStep(n)
+    e32.ForwardStep(n)
+    torch.cuda.synchronize()
+    worst = 0.0
+    for it in inst:
+        if it.smooth:  # (the untrained MLPs of this test are not meant to hold the shocks)
+            a, b = e32.solution(it), e64.solution(it)
+            assert torch.isfinite(a).all()
+            worst = max(worst, float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)))
+    with capsys.disabled():
+        print(f"\nFP32-bulk + learned-closure gas ensemble: worst relative L2 error vs FP64 on smooth members "
+              f"after {n} steps = {worst:.3e}")
+    assert 0.0 < worst < 1e-6

@@ -189,3 +189,19 @@ def test_oracle_thread_count_does_not_change_results():
         mod.rk3(2, 1e-3)
         outs.append(mod.get("solution"))
     np.testing.assert_array_equal(outs[0], outs[1])
+
+
+def test_gauss_n1_keeps_the_reference_fill_from_the_output_arrays():
+    """The reference's LegendreGauss at N = 1 (src/SELF_Quadrature.f90:217-222)
+    sets node 1 and weight 1 from its output arguments nodes(0) and
+    weights(0), not from the node it has just computed; with the zeroed arrays
+    Lagrange%Init passes, the second node is -0 with weight 0.  Library and
+    oracle keep that behaviour (so N = 1 Gauss models are not usable, as in
+    the reference); every other degree is the Gauss rule."""
+    import self_b200 as S
+    L = S.Lagrange(1)
+    assert L.controlPoints[0] == -np.sqrt(1.0 / 3.0) and L.controlPoints[1] == 0.0
+    assert L.qWeights[0] == 1.0 and L.qWeights[1] == 0.0
+    x, w = O.quadrature(1, O.GAUSS)
+    np.testing.assert_array_equal(x, L.controlPoints)
+    np.testing.assert_array_equal(w, L.qWeights)

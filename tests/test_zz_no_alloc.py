@@ -80,7 +80,11 @@ def _check_two_calls(S, mesh, N):
         assert _rel(out, prod) < TOL
 
 
-@pytest.mark.parametrize("N", [1, 3, 5, 7])
+# N = 1 is left out: the reference's LegendreGauss fills the second Gauss node
+# of N = 1 from its output arrays instead of the computed first node
+# (src/SELF_Quadrature.f90:217-222), so with zeroed arrays that quadrature has
+# a zero weight and every N = 1 Gauss model divides by it (the oracle too).
+@pytest.mark.parametrize("N", [2, 3, 5, 7])
 def test_noalloc_tendency_matches_engine_on_two_calls_in_a_row(N):
     import self_b200 as S
     mesh = S.Mesh2D(6, 5, periodic=(True, False), perturbation=0.04, bcid=S.BC_NONORMALFLOW,
