@@ -307,6 +307,14 @@ int selfgpu_model2d_sync(selfgpu_model2d* m);
  * then a fixed-order tree over the elements. */
 int selfgpu_model2d_entropy(selfgpu_model2d* m, double* entropy);
 
+/* Integral_MappedScalar2D (src/SELF_MappedData.f90:1270-1311): the sum of
+ * f(i,j,iVar,e) J(i,j,e) w_i w_j over the mesh for a device field interior
+ * (P,P,nVar,nEl) and device J (P,P,1,nEl), host qWeights (0:N); the result on
+ * the host (the stream is synchronised).  The reference integrates variable 4
+ * (hard-coded); iVar (1-based) chooses it here. */
+int selfgpu_integral_mapped_scalar2d(const double* interior, int iVar, int nVar, const double* J,
+                                     const double* qWeights, int N, int nEl, double* result, void* stream);
+
 /* Scan the solution for NaN/Inf on the device (SELFGPU_ERR_NONFINITE if any). */
 int selfgpu_model2d_check_finite(selfgpu_model2d* m);
 

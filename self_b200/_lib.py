@@ -41,6 +41,8 @@ _SIGS = {
     "selfgpu_model2d_sync": (c_int, [c_void_p]),
     "selfgpu_model2d_check_finite": (c_int, [c_void_p]),
     "selfgpu_model2d_entropy": (c_int, [c_void_p, ctypes.POINTER(c_double)]),
+    "selfgpu_integral_mapped_scalar2d": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_int, c_int,
+                                                 ctypes.POINTER(c_double), c_void_p]),
     "selfgpu_model2d_launch_count": (c_longlong, [c_void_p]),
     "selfgpu_model2d_persistent_launch_count": (c_longlong, [c_void_p]),
     "selfgpu_model2d_set_kernel": (c_int, [c_void_p, c_int]),

@@ -662,13 +662,16 @@ int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, f
   const StageLaunch saved = m->cfg;
   float best = 1e30f;
   StageLaunch bestCfg = saved;
-  for (int cand = 0; cand <= 9; ++cand) {
+  // consumer groups per CTA: up to 10 two-warp groups for P >= 6, up to 15
+  // one-warp groups for P <= 4 (TmaTraits::kMaxGroups)
+  const int maxCand = m->P <= 4 ? 14 : 9;
+  for (int cand = 0; cand <= maxCand; ++cand) {
     StageLaunch c = saved;
     if (cand == 0) {
       c.allowTma = false;
     } else {
       c.allowTma = true;
-      c.maxGroups = cand + 1;  // 2..10 consumer groups, capped by what fits
+      c.maxGroups = cand + 1;  // capped by what fits in shared memory
     }
     m->cfg = c;
     int tma = 0;
@@ -931,6 +934,52 @@ int selfgpu_model2d_entropy(selfgpu_model2d* m, double* entropy) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
   if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_entropy", e);
   *entropy = h;
+  return SELFGPU_OK;
+}
+
+// One block: every thread sums a strided subset of the elements, each element
+// in the reference's node order, then a shared-memory tree (fixed order).
+__global__ void __launch_bounds__(1024) k_integral_block(const double* __restrict__ f, int var, int nVar,
+                                                         const double* __restrict__ J, QwArr qw, int P, int nEl,
+                                                         double* out) {
+  __shared__ double part[1024];
+  const int PP = P * P;
+  double s = 0.0;
+  for (long long e = threadIdx.x; e < nEl; e += blockDim.x) {
+    const double* fe = f + (size_t)PP * (var + (size_t)nVar * e);
+    double se = 0.0;
+    for (int j = 0; j < P; ++j)
+      for (int i = 0; i < P; ++i) se = se + fe[i + P * j] * qw.w[i] * qw.w[j] * J[i + P * j + (size_t)PP * e];
+    s += se;
+  }
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = part[0];
+}
+
+int selfgpu_integral_mapped_scalar2d(const double* interior, int iVar, int nVar, const double* J,
+                                     const double* qWeights, int N, int nEl, double* result, void* stream) {
+  if (!interior || !J || !qWeights || !result || N < 1 || N > SELFGPU_MAX_N || nEl < 1 || nVar < 1 || iVar < 1 ||
+      iVar > nVar)
+    return set_error(SELFGPU_ERR_ARG, "selfgpu_integral_mapped_scalar2d: bad arguments");
+  QwArr w{};
+  for (int k = 0; k <= N; ++k) w.w[k] = qWeights[k];
+  double* d = nullptr;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMallocAsync(&d, sizeof(double), st);
+  if (e != cudaSuccess) return fail_cuda("selfgpu_integral_mapped_scalar2d", e);
+  k_integral_block<<<1, 1024, 0, st>>>(interior, iVar - 1, nVar, J, w, N + 1, nEl, d);
+  e = cudaGetLastError();
+  double h = 0.0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(d, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return fail_cuda("selfgpu_integral_mapped_scalar2d", e);
+  *result = h;
   return SELFGPU_OK;
 }
 

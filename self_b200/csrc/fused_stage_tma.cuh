@@ -90,7 +90,10 @@ struct TmaTraits {
   static constexpr int TS = trace_side_stride<P, NT, R>();
   static constexpr int TPE = (PP + 31) / 32 * 32;
   static_assert(TPE >= 4 * P, "the face phase gives each of the 4P face nodes its own thread");
-  static constexpr int kMaxGroups = 10;  // 640 threads: five warps per scheduler at 96 registers
+  // 640 threads (five warps per scheduler at 96 registers) for P >= 6; a
+  // P <= 4 element fits one warp, so up to 15 single-warp groups (named
+  // barriers 1..15; barrier 0 is the CTA-wide one)
+  static constexpr int kMaxGroups = (P <= 4) ? 15 : 10;
   static constexpr int kThreadsMax = kMaxGroups * TPE;
   // Per-group compute arrays (bulk type), laid out for conflict-free shared
   // accesses.  A 64-bit shared access is served per half-warp: two threads of
