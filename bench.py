@@ -313,7 +313,7 @@ def run_cpu_table():
     return rows
 
 
-def run_forms(steps=20, err_steps=500, n_instances=256):
+def run_forms(steps=500, err_steps=500, n_instances=256):
     """The ensemble workload: 256 seeded nonlinear ShallowWater instances
     (nx, ny ~ U{8..64}, N ~ U{3,5,7}, 4-Gaussian topography, reflecting walls,
     per-instance CFL-0.5 time step), advanced (a) one FP64 handle per instance,
@@ -531,9 +531,25 @@ def measure_c1():
     lsw.workSol.zero_()
     ms = _events_ms(lambda: lsw.ForwardStep(1000, 1e-4))
     lsw.CheckFinite()
-    return {"workload": "LinearShallowWater 10x10 walls N=7, gravity-wave release, 1000 RK3 steps, dt=1e-4, FP64 "
-                        "(19,200 DOF: launch-latency bound; graph-replayed steps)",
-            "value": 19200 * 1000 / (ms / 1e3), "unit": "DOF-updates/s", "ms_per_rk3_step": ms / 1000}
+    out = {"workload": "LinearShallowWater 10x10 walls N=7, gravity-wave release, 1000 RK3 steps, dt=1e-4, FP64 "
+                       "(19,200 DOF: launch-latency bound)",
+           "graph_replayed": {"value": 19200 * 1000 / (ms / 1e3), "unit": "DOF-updates/s",
+                              "ms_per_rk3_step": ms / 1000, "launches_per_solve": 3000}}
+    # all 3000 RK stages in one cooperative launch (selfgpu_model2d_set_multistep)
+    S.check(S.lib().selfgpu_model2d_set_multistep(lsw._h, 1))
+    lsw.SetSolution(q1)
+    lsw.workSol.zero_()
+    lsw.ForwardStep(10, 1e-4)
+    lsw.Sync()
+    lsw.SetSolution(q1)
+    lsw.workSol.zero_()
+    l0 = lsw.LaunchCount()
+    ms1 = _events_ms(lambda: lsw.ForwardStep(1000, 1e-4))
+    lsw.CheckFinite()
+    out["one_launch"] = {"value": 19200 * 1000 / (ms1 / 1e3), "unit": "DOF-updates/s",
+                         "ms_per_rk3_step": ms1 / 1000, "launches_per_solve": lsw.LaunchCount() - l0}
+    out["speedup_one_launch_vs_graph"] = ms / ms1
+    return out
 
 
 def measure_gas_ensemble(mlps, steps=100, n_instances=256):
@@ -604,7 +620,53 @@ def run_closure_forms():
     return out
 
 
-def run_one_form(name):
+def measure_kernel(model, Nd, nx, form, steps, kernel="persistent"):
+    """Diagnostic single-model run for profiling one stage kernel: a periodic
+    nx x nx mesh (perturbed 0.02 h) at degree Nd, a smooth state, `steps` RK3
+    steps after a warm-up; device time per RK stage and the algorithmic
+    bandwidth (the same byte count as the roofline)."""
+    import torch
+
+    import self_b200 as S
+    interp = S.Lagrange(Nd, S.GAUSS, Nd, S.UNIFORM)
+    mesh = S.Mesh2D(nx, nx, periodic=(True, True), perturbation=0.02)
+    geo = S.SEMQuad(interp, mesh)
+    cls = {"LSW": S.LinearShallowWater, "SW": S.ShallowWater, "CIG": S.CompressibleIdealGas2D}[model]
+    m = cls(mesh, geo, form={"fp64": S.FP64, "fp64_ref": S.FP64_REF, "fp32": S.FP32_BULK}[form])
+    S.lib().selfgpu_model2d_set_kernel(m._h, 1 if kernel == "persistent" else 0)
+    X, Y = geo.x[:, 0, :, :, 0], geo.x[:, 0, :, :, 1]
+    Pd = Nd + 1
+    nv = 4 if model == "CIG" else 3
+    q = torch.zeros((mesh.nElem, nv, Pd, Pd), device="cuda", dtype=torch.float64)
+    bump = 0.01 * torch.exp(-((X - 0.5) ** 2 + (Y - 0.5) ** 2) / 0.05)
+    if model == "CIG":
+        rho = 1.0 + 0.1 * torch.sin(2 * np.pi * X) * torch.sin(2 * np.pi * Y)
+        q[:, 0], q[:, 1], q[:, 2], q[:, 3] = rho * 0.5, rho * 0.3, rho, 2.5 + 0.17 * rho
+    elif model == "SW":
+        q[:, 2] = 1.0 + bump
+    else:
+        q[:, 2] = bump
+    m.SetSolution(q)
+    m.ForwardStep(2, 1e-5)
+    m.Sync()
+    ms = _events_ms(lambda: m.ForwardStep(steps, 1e-5))
+    m.CheckFinite()
+    NT = 9 if model == "CIG" else 3
+    A = {"CIG": 0, "SW": 8 * (2 * Pd * Pd + 4 * Pd), "LSW": 8 * (2 * Pd * Pd + 4 * Pd)}[model]
+    w = 4 if form == "fp32" else 8
+    b = w * (4 * nv * Pd * Pd + 8 * NT * Pd) + 8 * (5 * Pd * Pd + 12 * Pd) + A + 80
+    if form == "fp32":  # FP64 solution and RK register, FP32 traces
+        b = 8 * 4 * nv * Pd * Pd + 4 * 8 * NT * Pd + 8 * (5 * Pd * Pd + 12 * Pd) + A + 80
+    us = 1e3 * ms / (3 * steps)
+    return {"workload": f"{model} periodic {nx}x{nx} N={Nd} {form}, {kernel} kernel, {steps} RK3 steps",
+            "us_per_stage": us, "bytes_per_element_stage": b, "elements": mesh.nElem,
+            "algorithmic_GBps": b * mesh.nElem / us / 1e3,
+            "dof_updates_per_s": nv * Pd * Pd * mesh.nElem * steps / (ms / 1e3)}
+
+
+def run_one_form(name, args=None):
+    if name == "kernel":
+        return measure_kernel(args.model, args.N, args.nx, args.fp, args.kernel_steps, args.kernel)
     if name == "ensemble":
         return run_forms()
     if name == "gas_ensemble":
@@ -818,7 +880,12 @@ def main():
     ap.add_argument("--impl", default="selfgpu", choices=["selfgpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the ensemble / FP32-bulk form measurements")
-    ap.add_argument("--form", choices=["c1", "c2", "c4", "c5", "ensemble", "gas_ensemble"], default=None,
+    ap.add_argument("--model", default="CIG", choices=["LSW", "SW", "CIG"], help="--form kernel: model")
+    ap.add_argument("--N", type=int, default=7, help="--form kernel: degree")
+    ap.add_argument("--nx", type=int, default=128, help="--form kernel: elements per direction")
+    ap.add_argument("--fp", default="fp64", choices=["fp64", "fp64_ref", "fp32"], help="--form kernel: form")
+    ap.add_argument("--kernel-steps", type=int, default=5, help="--form kernel: timed RK3 steps")
+    ap.add_argument("--form", choices=["c1", "c2", "c4", "c5", "ensemble", "gas_ensemble", "kernel"], default=None,
                     help="run only this form's measurement and print its JSON (diagnostic mode)")
     ap.add_argument("--cpu-table", action="store_true",
                     help="print the CPU-baseline table of configs C1-C5 (oracle port) and exit")
@@ -829,7 +896,7 @@ def main():
         print(json.dumps(run_cpu_table()), flush=True)
         return
     if args.form:
-        print(json.dumps(run_one_form(args.form)), flush=True)
+        print(json.dumps(run_one_form(args.form, args)), flush=True)
         return
     from self_b200 import replicas as R
     rank, world, local_rank = R.init("gloo" if args.impl == "reference" else "nccl")

@@ -329,6 +329,16 @@ long long selfgpu_model2d_persistent_launch_count(const selfgpu_model2d* m);
  * one-CTA-per-element-group kernel. */
 int selfgpu_model2d_set_kernel(selfgpu_model2d* m, int persistent);
 
+/* Opt-in (enable = 1): selfgpu_model2d_rk3 runs all 3 nSteps RK stages as
+ * ONE cooperative launch (k_fused_steps: the per-element stage body, then a
+ * grid barrier before the next stage reads the traces other CTAs wrote) when
+ * the mesh's element groups fit one wave of resident CTAs -- small,
+ * launch-latency bound meshes such as the 10x10 gravity-wave release.  Larger
+ * meshes, a bound closure or halo fall back to graph-replayed steps.  The
+ * barrier waits are bounded like the persistent kernel's (set_wait_limit;
+ * SELFGPU_ERR_TIMEOUT from sync). */
+int selfgpu_model2d_set_multistep(selfgpu_model2d* m, int enable);
+
 /* Explicit launch configuration (what the autotuner picks): persistent 0/1
  * and the persistent kernel's consumer-group cap (0 = as many as fit). */
 int selfgpu_model2d_set_launch(selfgpu_model2d* m, int persistent, int groups);

@@ -46,6 +46,7 @@ _SIGS = {
     "selfgpu_model2d_launch_count": (c_longlong, [c_void_p]),
     "selfgpu_model2d_persistent_launch_count": (c_longlong, [c_void_p]),
     "selfgpu_model2d_set_kernel": (c_int, [c_void_p, c_int]),
+    "selfgpu_model2d_set_multistep": (c_int, [c_void_p, c_int]),
     "selfgpu_model2d_autotune": (c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int),
                                          ctypes.POINTER(ctypes.c_float)]),
     "selfgpu_model2d_set_launch": (c_int, [c_void_p, c_int, c_int]),

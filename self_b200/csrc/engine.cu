@@ -169,6 +169,8 @@ struct selfgpu_model2d {
   float* mlpB = nullptr;
   double* geo = nullptr;  // packed geometry records (persistent kernel)
   double* entropyBuf = nullptr;  // per-element entropy sums (nEl) and the total
+  bool multistep = false;         // rk3 as one cooperative launch where the mesh fits one wave
+  unsigned* stepBar = nullptr;    // grid-barrier counter of that launch
 
   size_t elemBytes() const { return form == SELFGPU_FP32_BULK ? sizeof(float) : sizeof(double); }
 
@@ -211,6 +213,44 @@ struct selfgpu_model2d {
     cudaError_t e = launch_stage_form(form, model, P, a, cfg, stream, &tma);
     tmaLaunches += tma;
     return e;
+  }
+
+  // nSteps RK3 steps as one cooperative launch of k_fused_steps from the
+  // current parities; cudaErrorCooperativeLaunchTooLarge when the element
+  // groups do not fit one wave of resident CTAs (the caller falls back).
+  cudaError_t launch_steps(double dt, int nSteps) {
+    cudaError_t e = cudaSuccess;
+    if (!stepBar) e = cudaMalloc(&stepBar, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemsetAsync(stepBar, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return e;
+    StepsArgs sa{};
+    sa.nSteps = nSteps;
+    sa.dt = dt;
+    for (int k = 0; k < 3; ++k) {
+      sa.rkA[k] = kRK3a[k];
+      sa.rkG[k] = kRK3g[k];
+    }
+    sa.tr[0] = tr[0];
+    sa.tr[1] = tr[1];
+    sa.vel[0] = vel[0];
+    sa.vel[1] = vel[1];
+    sa.cur = cur;
+    sa.vcur = vcur;
+    sa.bar = stepBar;
+    StageArgs a = base;
+    a.mode = MODE_RK;
+    switch (form) {
+      case SELFGPU_FP64: e = launch_steps_fp64(model, P, a, sa, cfg.numSMs, stream); break;
+      case SELFGPU_FP64_REF: e = launch_steps_fp64_ref(model, P, a, sa, cfg.numSMs, stream); break;
+      default: e = launch_steps_fp32(model, P, a, sa, cfg.numSMs, stream); break;
+    }
+    if (e != cudaSuccess) return e;
+    ++launches;
+    if ((3LL * nSteps) & 1) {  // three cache swaps per step
+      cur = 1 - cur;
+      if (model == SELFGPU_MODEL_SW) vcur = 1 - vcur;
+    }
+    return cudaSuccess;
   }
 
   void drop_graphs() {
@@ -355,7 +395,7 @@ int selfgpu_model2d_destroy(selfgpu_model2d* m) {
     if (m->vel[k]) cudaFree(m->vel[k]);
   }
   for (void* p : {(void*)m->avNu, (void*)m->avAct, (void*)m->avFallbacks, (void*)m->avH, m->avVisc, m->avVtr,
-                  (void*)m->mlpW, (void*)m->mlpB, (void*)m->geo, (void*)m->entropyBuf})
+                  (void*)m->mlpW, (void*)m->mlpB, (void*)m->geo, (void*)m->entropyBuf, (void*)m->stepBar})
     if (p) cudaFree(p);
   if (m->dflag) cudaFree(m->dflag);
   if (m->ownStream) cudaStreamDestroy(m->stream);
@@ -516,6 +556,13 @@ int selfgpu_model2d_rk3(selfgpu_model2d* m, double dt, int nSteps) {
     e = m->prologue();
     if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_rk3", e);
   }
+  if (m->multistep && nSteps > 0 && m->avMode == AV_OFF && m->nHalo == 0 && !m->base.debugStarve) {
+    e = m->launch_steps(dt, nSteps);
+    if (e == cudaSuccess) return SELFGPU_OK;
+    cudaGetLastError();
+    if (e != cudaErrorCooperativeLaunchTooLarge) return fail_cuda("selfgpu_model2d_rk3: multi-step launch", e);
+    // the mesh does not fit one wave: graph-replayed steps below
+  }
   if (!(dt == m->graphDt)) m->drop_graphs();
   for (int s = 0; s < nSteps; ++s) {
     cudaGraphExec_t& g = m->graph[m->cur][m->vcur];
@@ -590,6 +637,12 @@ int selfgpu_model2d_inject_stall(selfgpu_model2d* m, int enable) {
   if (!m) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_inject_stall: null handle");
   m->base.debugStarve = enable ? 1 : 0;
   m->drop_graphs();
+  return SELFGPU_OK;
+}
+
+int selfgpu_model2d_set_multistep(selfgpu_model2d* m, int enable) {
+  if (!m) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_multistep: null handle");
+  m->multistep = enable != 0;
   return SELFGPU_OK;
 }
 

@@ -400,13 +400,35 @@ struct Smem {
   R vel[Phys::kLaggedVelocity ? 2 : 1][4][2][P];
 };
 
-template <int P, class Phys, typename R, int EPB>
-__global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
+// The per-stage part of a launch (mode, RK coefficients, the trace-cache
+// halves read and written); everything else comes from StageArgs.
+struct StageVar {
+  int mode;
+  double rk_a, rk_gdt, rk_g;
+  const void* trIn;
+  void* trOut;
+  const void* velIn;
+  void* velOut;
+};
+
+// A load from the trace cache.  kCoherent = true (the multi-stage kernel,
+// where other CTAs of the same launch wrote the data a grid barrier ago)
+// reads through L2 only, never a possibly stale L1 line.
+template <bool kCoherent, typename R>
+__device__ __forceinline__ R ld_trace(const R* p) {
+  if constexpr (kCoherent) return __ldcg(p);
+  else return *p;
+}
+
+// One stage over the CTA's EPB element slots (one thread per node): the body
+// of k_fused_stage, shared with the multi-stage kernel k_fused_steps.  The
+// operator matrices are already in shared memory (sdg, sb, srw).
+template <int P, class Phys, typename R, int EPB, bool kCoherent>
+__device__ __forceinline__ void fused_stage_group(const StageArgs& a, const StageVar& sv, Smem<P, Phys, R>* sm_all,
+                                                  const double* sdg, const double* sb, const double* srw) {
   constexpr int NV = Phys::NV, NT = Phys::NT, NF = Phys::NF, PP = P * P, N = P - 1;
   constexpr int TS = trace_side_stride<P, NT, R>();
   using S = Smem<P, Phys, R>;
-  __shared__ S sm_all[EPB];
-  __shared__ double sdg[PP], sb[2 * P], srw[P];
 
   const int tid = threadIdx.x;
   const int slot = tid / PP;
@@ -414,14 +436,10 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
   const int i = t % P, j = t / P;
   S& sm = sm_all[slot];
 
-  for (int k = tid; k < PP; k += blockDim.x) sdg[k] = a.dgM[k];
-  for (int k = tid; k < 2 * P; k += blockDim.x) sb[k] = a.bM[k];
-  for (int k = tid; k < P; k += blockDim.x) srw[k] = a.qw[k];
-
   const long long e = (long long)blockIdx.x * EPB + slot;
   const bool live = e < a.nEl;
-  const R* trIn = reinterpret_cast<const R*>(a.trIn);
-  R* trOut = reinterpret_cast<R*>(a.trOut);
+  const R* trIn = reinterpret_cast<const R*>(sv.trIn);
+  R* trOut = reinterpret_cast<R*>(sv.trOut);
   const long long gnode = t + (long long)PP * e;
 
   if (live) {
@@ -431,7 +449,7 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
     Phys::template node<R>(f, a);
 #pragma unroll
     for (int v = 0; v < NF; ++v) sm.fld[v][t] = f[v];
-    if (a.mode != MODE_TRACES) {
+    if (sv.mode != MODE_TRACES) {
       double na[3];
       node_aux_global<Phys>(a, t, e, PP, na);
       R Fx[NV], Fy[NV];
@@ -458,26 +476,26 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
         if (si[4] == 0) {
           const long long e2 = si[2] - 1;
           const int s2 = si[3] / 10 - 1, flip = si[3] % 10;
-          val = trIn[(flip ? N - ii : ii) + P * fi + (long long)TS * (s2 + 4 * e2)];
+          val = ld_trace<kCoherent>(trIn + (flip ? N - ii : ii) + P * fi + (long long)TS * (s2 + 4 * e2));
         }
         sm.ext[s1][fi][ii] = val;
         // own traces of this stage's solution: the trace cache holds them (the
         // previous launch formed them from the same values with the same sums)
-        sm.own[s1][fi][ii] = trIn[ii + P * fi + (long long)TS * (s1 + 4 * e)];
+        sm.own[s1][fi][ii] = ld_trace<kCoherent>(trIn + ii + P * fi + (long long)TS * (s1 + 4 * e));
       }
       if constexpr (Phys::kLaggedVelocity) {
-        const R* vIn = reinterpret_cast<const R*>(a.velIn);
+        const R* vIn = reinterpret_cast<const R*>(sv.velIn);
         for (int k = t; k < 16 * P; k += PP) {
           const int ii = k % P, d = (k / P) % 2, s1 = (k / (2 * P)) % 4, which = k / (8 * P);
           R val = (R)0;
           if (which == 0) {
-            val = vIn[ii + P * (d + 2 * (s1 + 4 * e))];
+            val = ld_trace<kCoherent>(vIn + ii + P * (d + 2 * (s1 + 4 * e)));
           } else {
             const int* si = a.sideInfo + 5 * (s1 + 4 * e);
             if (si[4] == 0) {  // velocity%extBoundary is only ever set by the exchange (H8)
               const long long e2 = si[2] - 1;
               const int s2 = si[3] / 10 - 1, flip = si[3] % 10;
-              val = vIn[(flip ? N - ii : ii) + P * (d + 2 * (s2 + 4 * e2))];
+              val = ld_trace<kCoherent>(vIn + (flip ? N - ii : ii) + P * (d + 2 * (s2 + 4 * e2)));
             }
           }
           sm.vel[which][s1][d][ii] = val;
@@ -485,7 +503,7 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
       }
     }
   }
-  if (a.mode != MODE_TRACES) {
+  if (sv.mode != MODE_TRACES) {
     __syncthreads();
     // 4P face nodes per element; for P <= 3 there are fewer node threads (P*P)
     if (live)
@@ -512,7 +530,7 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
           velL[1] = sm.vel[0][s1][1][ii];
           velR[0] = sm.vel[1][s1][0][ii];
           velR[1] = sm.vel[1][s1][1][ii];
-          R* vOut = reinterpret_cast<R*>(a.velOut);  // read by the next stage
+          R* vOut = reinterpret_cast<R*>(sv.velOut);  // read by the next stage
           vOut[ii + P * (0 + 2 * (s1 + 4 * e))] = L[0] / L[2];
           vOut[ii + P * (1 + 2 * (s1 + 4 * e))] = L[1] / L[2];
         }
@@ -558,24 +576,24 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
           dsdt = Src[v] - (double)d * rJ;
         }
         const long long gi = t + (long long)PP * (v + NV * e);
-        if (a.mode == MODE_TENDENCY) {
+        if (sv.mode == MODE_TENDENCY) {
           a.dSdt[gi] = dsdt;
         } else {
-          const double Gn = a.rk_a * a.G[gi] + dsdt;
+          const double Gn = sv.rk_a * a.G[gi] + dsdt;
           a.G[gi] = Gn;
-          const double qn = qd[v] + (a.dtElem ? a.rk_g * a.dtElem[e] : a.rk_gdt) * Gn;
+          const double qn = qd[v] + (a.dtElem ? sv.rk_g * a.dtElem[e] : sv.rk_gdt) * Gn;
           a.q[gi] = qn;
           f[v] = (R)qn;
         }
       }
-      if (a.mode == MODE_RK) {
+      if (sv.mode == MODE_RK) {
         // only this thread reads node t of fld in this phase, so it may overwrite it
         Phys::template node<R>(f, a);
 #pragma unroll
         for (int v = 0; v < NF; ++v) sm.fld[v][t] = f[v];
       }
     }
-    if (a.mode == MODE_TENDENCY) return;
+    if (sv.mode == MODE_TENDENCY) return;
   }
   __syncthreads();
   // traces of the (updated) solution -> trace cache: one task per (field,
@@ -600,18 +618,107 @@ __global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
   if constexpr (Phys::kLaggedVelocity) {
     // Start of a run: the stage-lagged velocity traces equal those of this
     // solution (SetSolution leaves solution%boundary = BoundaryInterp(solution)).
-    if (a.mode == MODE_TRACES && a.velOut != nullptr) {
+    if (sv.mode == MODE_TRACES && sv.velOut != nullptr) {
       __syncthreads();
       if (live)
         for (int k = t; k < 4 * P; k += PP) {
           const int s1 = k / P, ii = k % P;
-          R* vOut = reinterpret_cast<R*>(a.velOut);
+          R* vOut = reinterpret_cast<R*>(sv.velOut);
           const R H = o[ii + P * 2 + TS * s1];
           vOut[ii + P * (0 + 2 * (s1 + 4 * e))] = o[ii + P * 0 + TS * s1] / H;
           vOut[ii + P * (1 + 2 * (s1 + 4 * e))] = o[ii + P * 1 + TS * s1] / H;
         }
     }
   }
+}
+
+
+template <int P, class Phys, typename R, int EPB>
+__global__ void __launch_bounds__(EPB* P* P) k_fused_stage(const StageArgs a) {
+  constexpr int PP = P * P;
+  __shared__ Smem<P, Phys, R> sm_all[EPB];
+  __shared__ double sdg[PP], sb[2 * P], srw[P];
+  for (int k = threadIdx.x; k < PP; k += blockDim.x) sdg[k] = a.dgM[k];
+  for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) sb[k] = a.bM[k];
+  for (int k = threadIdx.x; k < P; k += blockDim.x) srw[k] = a.qw[k];
+  const StageVar sv{a.mode, a.rk_a, a.rk_gdt, a.rk_g, a.trIn, a.trOut, a.velIn, a.velOut};
+  fused_stage_group<P, Phys, R, EPB, false>(a, sv, sm_all, sdg, sb, srw);
+}
+
+// ------------------------------------------------- multi-stage (one launch)
+// Arguments of k_fused_steps: nSteps Williamson RK3 steps of size dt from
+// the trace-cache halves cur / vcur, with a grid barrier counter.
+struct StepsArgs {
+  int nSteps;
+  double dt;
+  double rkA[3], rkG[3];
+  const void* tr[2];
+  const void* vel[2];
+  int cur, vcur;
+  unsigned* bar;  // zero at launch; counts CTA arrivals over all barriers
+};
+
+// Grid-wide barrier number k (1-based) of a launch whose CTAs are all
+// resident (cooperative launch).  Bounded: a CTA that waits longer than
+// `cycles` sets the error word and returns false (the launch then stops).
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned k, long long cycles, int* err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(bar, 1u);
+    const unsigned target = k * gridDim.x;
+    int ok = 1;
+    const long long t0 = clock64();
+    while (true) {
+      unsigned v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+      if (v >= target) break;
+      if (clock64() - t0 > cycles) {
+        ok = 0;
+        if (err) atomicExch(err, 1);
+        break;
+      }
+      __nanosleep(32);
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// All RK stages of nSteps steps in one cooperative launch, for meshes whose
+// element groups fit one wave of resident CTAs (the small, launch-latency
+// bound cases): each stage is the k_fused_stage body over the CTA's elements,
+// then a grid barrier before the next stage reads the traces other CTAs
+// wrote.  Trace reads go through L2 (ld_trace<true>).
+template <int P, class Phys, typename R, int EPB>
+__global__ void __launch_bounds__(EPB* P* P) k_fused_steps(const StageArgs a, const StepsArgs sa) {
+  constexpr int PP = P * P;
+  __shared__ Smem<P, Phys, R> sm_all[EPB];
+  __shared__ double sdg[PP], sb[2 * P], srw[P];
+  for (int k = threadIdx.x; k < PP; k += blockDim.x) sdg[k] = a.dgM[k];
+  for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) sb[k] = a.bM[k];
+  for (int k = threadIdx.x; k < P; k += blockDim.x) srw[k] = a.qw[k];
+  int cur = sa.cur, vcur = sa.vcur;
+  unsigned k = 0;
+  for (int s = 0; s < sa.nSteps; ++s)
+    for (int m = 0; m < 3; ++m) {
+      StageVar sv;
+      sv.mode = MODE_RK;
+      sv.rk_a = sa.rkA[m];
+      sv.rk_gdt = sa.rkG[m] * sa.dt;
+      sv.rk_g = sa.rkG[m];
+      sv.trIn = sa.tr[cur];
+      sv.trOut = const_cast<void*>(sa.tr[1 - cur]);
+      sv.velIn = sa.vel[vcur];
+      sv.velOut = const_cast<void*>(sa.vel[1 - vcur]);
+      fused_stage_group<P, Phys, R, EPB, true>(a, sv, sm_all, sdg, sb, srw);
+      cur ^= 1;
+      if constexpr (Phys::kLaggedVelocity) vcur ^= 1;
+      if (!grid_barrier(sa.bar, ++k, a.waitCycles, a.err)) return;
+    }
 }
 
 }  // namespace selfgpu

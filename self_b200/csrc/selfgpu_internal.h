@@ -45,6 +45,12 @@ cudaError_t launch_stage_fp64_ref(int model, int P, const StageArgs& a, const St
                                   int* usedTma);
 cudaError_t launch_stage_fp32(int model, int P, const StageArgs& a, const StageLaunch& L, cudaStream_t st,
                               int* usedTma);
+// nSteps RK3 steps in one cooperative launch (k_fused_steps), per form
+struct StepsArgs;
+cudaError_t launch_steps_fp64(int model, int P, const StageArgs& a, const StepsArgs& sa, int numSMs, cudaStream_t st);
+cudaError_t launch_steps_fp64_ref(int model, int P, const StageArgs& a, const StepsArgs& sa, int numSMs,
+                                  cudaStream_t st);
+cudaError_t launch_steps_fp32(int model, int P, const StageArgs& a, const StepsArgs& sa, int numSMs, cudaStream_t st);
 // Artificial-viscosity closure (av_closure.cuh).
 struct AvArgs;
 // closure: the viscosity kernel and the viscous-term kernel of one stage

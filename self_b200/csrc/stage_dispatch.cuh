@@ -88,6 +88,48 @@ cudaError_t launch_P(int P, const StageArgs& a, const StageLaunch& L, cudaStream
   }
 }
 
+// One cooperative launch of k_fused_steps; cudaErrorCooperativeLaunchTooLarge
+// when the element groups do not fit one wave of resident CTAs.
+template <int P, class Phys, typename R>
+cudaError_t launch_steps_one(const StageArgs& a, const StepsArgs& sa, int numSMs, cudaStream_t st) {
+  constexpr int EPB = elems_per_block<P, Phys, R>();
+  const int grid = (a.nEl + EPB - 1) / EPB;
+  int perSM = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_fused_steps<P, Phys, R, EPB>, EPB * P * P, 0);
+  if (e != cudaSuccess) return e;
+  if ((long long)perSM * numSMs < grid) return cudaErrorCooperativeLaunchTooLarge;
+  StageArgs aa = a;
+  StepsArgs ss = sa;
+  void* args[] = {&aa, &ss};
+  return cudaLaunchCooperativeKernel((const void*)k_fused_steps<P, Phys, R, EPB>, dim3(grid), dim3(EPB * P * P),
+                                     args, 0, st);
+}
+
+template <class Phys, typename R>
+cudaError_t launch_steps_P(int P, const StageArgs& a, const StepsArgs& sa, int numSMs, cudaStream_t st) {
+  switch (P) {
+    case 2: return launch_steps_one<2, Phys, R>(a, sa, numSMs, st);
+    case 3: return launch_steps_one<3, Phys, R>(a, sa, numSMs, st);
+    case 4: return launch_steps_one<4, Phys, R>(a, sa, numSMs, st);
+    case 5: return launch_steps_one<5, Phys, R>(a, sa, numSMs, st);
+    case 6: return launch_steps_one<6, Phys, R>(a, sa, numSMs, st);
+    case 7: return launch_steps_one<7, Phys, R>(a, sa, numSMs, st);
+    case 8: return launch_steps_one<8, Phys, R>(a, sa, numSMs, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <typename R>
+cudaError_t launch_steps_impl(int model, int P, const StageArgs& a, const StepsArgs& sa, int numSMs,
+                              cudaStream_t st) {
+  switch (model) {
+    case SELFGPU_MODEL_LSW: return launch_steps_P<PhysLSW, R>(P, a, sa, numSMs, st);
+    case SELFGPU_MODEL_SW: return launch_steps_P<PhysSW, R>(P, a, sa, numSMs, st);
+    case SELFGPU_MODEL_CIG: return launch_steps_P<PhysCIG, R>(P, a, sa, numSMs, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 template <typename R>
 cudaError_t launch_stage_impl(int model, int P, const StageArgs& a, const StageLaunch& L, cudaStream_t st,
                               int* usedTma) {

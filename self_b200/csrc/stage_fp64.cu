@@ -52,4 +52,7 @@ cudaError_t launch_closure_features(const double* q, int P, int nEl, const AvArg
       return cudaErrorInvalidValue;
   }
 }
+cudaError_t launch_steps_fp64_ref(int model, int P, const StageArgs& a, const StepsArgs& sa, int numSMs, cudaStream_t st) {
+  return launch_steps_impl<double>(model, P, a, sa, numSMs, st);
+}
 }  // namespace selfgpu

@@ -12,4 +12,7 @@ cudaError_t launch_stage_fp64(int model, int P, const StageArgs& a, const StageL
                               int* usedTma) {
   return launch_stage_impl<double>(model, P, a, L, st, usedTma);
 }
+cudaError_t launch_steps_fp64(int model, int P, const StageArgs& a, const StepsArgs& sa, int numSMs, cudaStream_t st) {
+  return launch_steps_impl<double>(model, P, a, sa, numSMs, st);
+}
 }  // namespace selfgpu

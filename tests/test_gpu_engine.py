@@ -516,3 +516,81 @@ def test_entropy_matches_oracle(model, mesh_kind):
         e_o = mod_o.entropy()
         e = mod.CalculateEntropy()
         assert e_o != 0.0 and abs(e - e_o) <= 1e-12 * abs(e_o), (k, e, e_o)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_c1_one_launch_1000_steps(form):
+    """The gravity-wave release (LSW 10x10 walls, N = 7, dt = 1e-4) with all
+    3000 RK stages in one cooperative launch: equal to the oracle bit for bit
+    in the reference-rounding form, within 1e-12 in the production form."""
+    import self_b200 as S
+    N, dt, steps = 7, 1e-4, 1000
+    kw = dict(nx=10, ny=10, bcid=O.BC_NONORMALFLOW, amp=0.0)
+    om, pm = C.oracle_mesh(kw), C.product_mesh(kw)
+    mod_o = O.Model(C.MODELS["LSW"], N, om)
+    geo_o = O.Geometry(N, om)
+    geo = S.SEMQuad(S.Lagrange(N, S.GAUSS, N, S.UNIFORM), pm)
+    mod = S.LinearShallowWater(pm, geo, form=form)
+    S.check(S.lib().selfgpu_model2d_set_multistep(mod._h, 1))
+    X, Y = geo_o.x[0, :, :, 0, :], geo_o.x[1, :, :, 0, :]
+    P = N + 1
+    q0 = np.zeros((P, P, 3, X.shape[2]), order="F")
+    q0[:, :, 2] = 0.01 * np.exp(-((X - 0.5) ** 2 + (Y - 0.5) ** 2) / 0.01)
+    H = np.ones((P, P, 1, X.shape[2]), order="F")
+    f = np.zeros((P, P, 1, X.shape[2]), order="F")
+    for m_ in (mod_o,):
+        m_.set("H", H)
+        m_.set("fCori", f)
+        m_.set("solution", q0)
+    mod.SetBathymetry(H)
+    mod.SetCoriolis(f)
+    mod.SetSolution(q0)
+    l0 = mod.LaunchCount()
+    mod.ForwardStep(steps, dt)
+    mod.Sync()
+    assert mod.LaunchCount() - l0 <= 2  # the trace prologue and the one multi-stage launch
+    mod_o.rk3(steps, dt)
+    ref = mod_o.get("solution", q0.shape)
+    got = S.to_host(mod.solution).reshape(ref.shape, order="F")
+    assert np.isfinite(got).all()
+    if form == S.FP64_REF:
+        np.testing.assert_array_equal(got, ref)
+    else:
+        for v in range(3):
+            assert C.rel_err(got[:, :, v], ref[:, :, v]) < TOL, (v, C.rel_err(got[:, :, v], ref[:, :, v]))
+
+
+@pytest.mark.parametrize("model,mesh_kind,N", [("SW", "flipped", 5), ("CIG", "prescribed", 4), ("LSW", "periodic", 3)])
+def test_one_launch_steps_match_oracle(model, mesh_kind, N):
+    """One cooperative launch for several RK3 steps, over two calls (odd step
+    counts, so the trace-cache parity flips between them), for every model:
+    the reference-rounding form equals the oracle bit for bit."""
+    import self_b200 as S
+    mod_o, mod, _, _ = build_pair(model, mesh_kind, N, seed=8, form=S.FP64_REF)
+    S.check(S.lib().selfgpu_model2d_set_multistep(mod._h, 1))
+    mod.ForwardStep(3, 1e-3)
+    mod.ForwardStep(4, 1e-3)
+    mod.Sync()
+    mod_o.rk3(7, 1e-3)
+    ref = mod_o.get("solution", (N + 1, N + 1, mod.nVar, mod.nElem))
+    np.testing.assert_array_equal(S.to_host(mod.solution).reshape(ref.shape, order="F"), ref)
+
+
+def test_one_launch_falls_back_on_a_mesh_larger_than_one_wave():
+    """A mesh whose element groups exceed one wave of resident CTAs runs the
+    graph-replayed steps instead, with the same result."""
+    import self_b200 as S
+    outs = []
+    for ms in (1, 0):
+        mesh = S.Mesh2D(96, 96, periodic=(True, True))
+        geo = S.SEMQuad(S.Lagrange(7), mesh)
+        mod = S.CompressibleIdealGas2D(mesh, geo, form=S.FP64_REF)
+        S.check(S.lib().selfgpu_model2d_set_multistep(mod._h, ms))
+        X, Y = geo.x[..., 0], geo.x[..., 1]
+        rho = 1.0 + 0.1 * torch.sin(2 * np.pi * X) * torch.sin(2 * np.pi * Y)
+        q = torch.stack([rho * 0.5, rho * 0.3, rho, 2.5 + 0.17 * rho], dim=1)[:, :, 0].contiguous()
+        mod.SetSolution(q)
+        mod.ForwardStep(3, 1e-4)
+        mod.Sync()
+        outs.append(mod.solution.clone())
+    assert torch.equal(outs[0], outs[1])
