@@ -8,7 +8,7 @@
 2. ``oracle_regression.npz`` -- outputs of the CPU oracle on small fixed cases,
    so a later change to the oracle that alters its numbers is caught.
 
-Usage: python tests/golden/make_golden.py [path-to-SELF-checkout]
+Usage: python tests/golden/make_golden.py <path-to-SELF-checkout>
 """
 import json
 import os
@@ -97,7 +97,9 @@ def regression():
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the SELF source tree>")
+    ref_root = sys.argv[1]
     with open(os.path.join(HERE, "reference_meshes.json"), "w") as f:
         json.dump(meshes(ref_root), f)
     np.savez_compressed(os.path.join(HERE, "oracle_regression.npz"), **regression())

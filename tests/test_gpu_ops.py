@@ -2,7 +2,9 @@
 
 Each wrapper is called exactly as SELF's Fortran calls it: through the C ABI
 with pointers to device pointers.  Bit-exact for the copy/exchange operators,
-1e-13 relative for the arithmetic ones (FMA contraction on the device).
+1e-13 relative for the arithmetic ones (the wrappers are built without
+multiply-add contraction, in the reference's order; the margin covers the
+device's libm transcendentals where a wrapper uses them).
 """
 import numpy as np
 import pytest
