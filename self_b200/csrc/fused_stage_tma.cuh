@@ -88,14 +88,20 @@ template <int P, class Phys, typename R>
 struct TmaTraits {
   static constexpr int PP = P * P, NV = Phys::NV, NT = Phys::NT, NF = Phys::NF;
   static constexpr int TS = trace_side_stride<P, NT, R>();
-  static constexpr int TPE = (PP + 31) / 32 * 32;
-  static_assert(TPE >= 4 * P, "the face phase gives each of the 4P face nodes its own thread");
-  // 640 threads (five warps per scheduler at 96 registers) for P >= 6; a
-  // P <= 4 element fits one warp, so up to 15 single-warp groups (named
-  // barriers 1..15; barrier 0 is the CTA-wide one)
-  static constexpr int kMaxGroups = (P <= 4) ? 15 : 10;
+  // Elements per group: a P = 4 element (16 nodes) would leave half of its
+  // warp's lanes idle, so its groups take two elements at a time (a tile of
+  // consecutive elements).  P = 6 stays at one element per two-warp group:
+  // two elements in three warps measured slower (six groups at 96 registers
+  // with spills against ten groups).  The code serves any EPG.
+  static constexpr int EPG = (P == 4) ? 2 : 1;
+  static constexpr int TPE = (EPG * PP + 31) / 32 * 32;  // threads per group
+  static_assert(TPE >= EPG * 4 * P, "the face phase gives each of the 4P face nodes its own thread");
+  // 640 threads (five warps per scheduler at 96 registers) for P = 6 and 8,
+  // up to 15 single-warp groups for P <= 4 (named barriers 1..15; barrier 0
+  // is the CTA-wide one)
+  static constexpr int kMaxGroups = (P <= 4) ? 15 : (P == 6 && EPG == 2 ? 6 : 10);
   static constexpr int kThreadsMax = kMaxGroups * TPE;
-  // Per-group compute arrays (bulk type), laid out for conflict-free shared
+  // Per-element compute arrays (bulk type), laid out for conflict-free shared
   // accesses.  A 64-bit shared access is served per half-warp: two threads of
   // a half-warp that touch different words of one bank pair (8-byte word
   // index mod 16) cost an extra pass.
@@ -107,18 +113,25 @@ struct TmaTraits {
   //    rows to P + 1.
   //  * boundary-normal flux [4][SS]: sides SS values apart, SS * sizeof(R) =
   //    64 (mod 128).
+  // With two elements per group their arrays follow each other (EB values
+  // apart), and the divergence sums go to a separate array (NV P^2 per
+  // element) instead of replacing the xi flux, since one element's
+  // divergence threads may then span two warps.
   static constexpr bool kSwz = (P == 8);
   static constexpr int RS = kSwz ? P : P + 1;
   static constexpr int FS = kSwz ? PP + 8 : P * RS;
   static constexpr int kU = (NF * FS > 2 * NV * PP) ? NF * FS : 2 * NV * PP;  // node fields alias the fluxes
   static constexpr int SS = side_stride(NV * P, (int)sizeof(R));
-  static constexpr int groupBytes = (int)(((kU + 4 * SS) * sizeof(R) + 127) / 128 * 128);
+  static constexpr int EB = kU + 4 * SS;
+  static constexpr int kDiv = EPG > 1 ? NV * PP : 0;  // separate divergence sums per element
+  static constexpr int groupBytes = (int)(((EPG * (EB + kDiv)) * sizeof(R) + 127) / 128 * 128);
   // Weak-divergence volume sums: one thread per 2x2 block of nodes and pair
-  // of variables, all in one warp.  The xi flux rows are stored with their
-  // value pairs XOR-swizzled per row pair (P/2 a power of two), so that the
-  // paired loads of a quarter-warp fall into distinct banks.
+  // of variables.  The xi flux rows are stored with their value pairs
+  // XOR-swizzled per row pair (P/2 a power of two), so that the paired loads
+  // of a quarter-warp fall into distinct banks.
   static constexpr int HB = P / 2, NVP = (NV + 1) / 2, NB = HB * HB * NVP;
-  static_assert(NB <= 32, "the divergence blocks fit one warp");
+  static_assert(EPG > 1 || NB <= 32, "one element's divergence blocks fit one warp");
+  static_assert(EPG * NB <= TPE, "every divergence block has its own thread");
   static constexpr bool kSwzF = (HB & (HB - 1)) == 0;
   // position of value m in row j of the xi flux
   __device__ __forceinline__ static int f0pos(int m, int j) {
@@ -137,7 +150,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     k_fused_stage_tma(const StageArgs a, const TmaPlan pl) {
   using T = TmaTraits<P, Phys, R>;
   constexpr int NV = T::NV, NT = T::NT, NF = T::NF, PP = T::PP, TS = T::TS, TPE = T::TPE, N = P - 1;
-  constexpr int FS = T::FS, SS = T::SS;
+  constexpr int FS = T::FS, SS = T::SS, EPG = T::EPG, EB = T::EB;
   constexpr bool kLSW = (NV == 3 && !Phys::kLaggedVelocity);
   constexpr bool kSW = Phys::kLaggedVelocity;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -146,7 +159,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   double* sdg = reinterpret_cast<double*>(smem + pl.oMats);
   double* sb = sdg + PP;
   double* sqw = sb + 2 * P;
-  double* sqwr = sqw + P;  // 1/w (used by the FP32-bulk form)
+  double* sqwr = sqw + P;  // 1/w (the FP32-bulk and production FP64 forms)
   volatile int* gflag = reinterpret_cast<volatile int*>(smem + pl.oFlags);
   unsigned char* slots = smem + pl.oSlots;
 
@@ -171,18 +184,24 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   asm volatile("griddepcontrol.wait;" ::: "memory");
 
+  // Work items are tiles of EPG consecutive elements; the CTA takes tiles
+  // blockIdx.x, blockIdx.x + gridDim.x, ...
+  const long long nTiles = ((long long)a.nEl + EPG - 1) / EPG;
   const long long nMine =
-      (long long)blockIdx.x < a.nEl ? ((long long)a.nEl - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+      (long long)blockIdx.x < nTiles ? (nTiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
   const bool rk = (a.mode == MODE_RK);
   const int g = threadIdx.x / TPE;
   const int t = threadIdx.x % TPE;
   if (g >= C) return;
 
-  // Group g consumes the CTA's elements g, g + C, g + 2C, ... through its two
-  // buffers; its thread 0 issues the copies of local element jj + 2 into the
-  // buffer that element jj has just released.
+  // Group g consumes the CTA's tiles g, g + C, g + 2C, ... through its two
+  // buffers; its thread 0 issues the copies of local tile jj + 2 into the
+  // buffer that tile jj has just released.  Every piece of a tile is
+  // contiguous in global memory (element-major arrays), so a tile is still
+  // one bulk copy per piece.
   const uint32_t qb = NV * PP * 8, gb = geo_record_doubles<P>() * 8, ob = 4 * TS * sizeof(R);
-  uint32_t xb[5] = {0, 0, 0, 0, 0};
+  const uint32_t vb = kSW ? 8 * P * sizeof(R) : 0;
+  uint32_t xb[5] = {0, 0, 0, 0, 0};  // per element
   if constexpr (kLSW) {
     xb[0] = PP * 8;
     xb[1] = 4 * P * 8;
@@ -195,35 +214,46 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     xb[1] = a.fld[1] ? PP * 8 : 0;
     xb[2] = xb[3] = xb[4] = a.fld[2] ? 16 * P * 8 : 0;
   }
+  auto tile_live = [&](long long k) -> int {  // live elements of the CTA's local tile k
+    const long long e0 = (blockIdx.x + k * gridDim.x) * EPG;
+    const long long r = (long long)a.nEl - e0;
+    return r < EPG ? (int)r : EPG;
+  };
   auto issue = [&](long long jj) {  // thread 0 only
     const long long k = g + jj * C;
     if (k >= nMine) return;
     const int buf = (int)(jj & 1);
-    const long long e = blockIdx.x + k * gridDim.x;
+    const long long e = (blockIdx.x + k * gridDim.x) * EPG;  // first element of the tile
+    const uint32_t nl = (EPG == 1) ? 1u : (uint32_t)tile_live(k);
     unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
     uint64_t* bar = &full[2 * g + buf];
-    uint32_t bytes = qb + gb + ob + xb[0] + xb[1] + xb[2] + xb[3] + xb[4];
-    if constexpr (kSW) bytes += 8 * P * sizeof(R);
+    const uint32_t bytes = nl * (qb + gb + ob + vb + xb[0] + xb[1] + xb[2] + xb[3] + xb[4]);
     mbar_arrive_expect_tx(bar, bytes);
     if (a.debugStarve && blockIdx.x == 0 && k == 0) return;
     const R* trIn = reinterpret_cast<const R*>(a.trIn);
-    bulk_g2s(sl + pl.oQ, a.q + (size_t)e * NV * PP, qb, bar);
-    bulk_g2s(sl + pl.oDsdx, a.geo + (size_t)e * geo_record_doubles<P>(), gb, bar);
-    bulk_g2s(sl + pl.oOwn, trIn + (size_t)4 * TS * e, ob, bar);
+    bulk_g2s(sl + pl.oQ, a.q + (size_t)e * NV * PP, nl * qb, bar);
+    bulk_g2s(sl + pl.oDsdx, a.geo + (size_t)e * geo_record_doubles<P>(), nl * gb, bar);
+    bulk_g2s(sl + pl.oOwn, trIn + (size_t)4 * TS * e, nl * ob, bar);
     if constexpr (kSW)
-      bulk_g2s(sl + pl.oVelOwn, reinterpret_cast<const R*>(a.velIn) + (size_t)e * 8 * P, 8 * P * sizeof(R), bar);
+      bulk_g2s(sl + pl.oVelOwn, reinterpret_cast<const R*>(a.velIn) + (size_t)e * 8 * P, nl * vb, bar);
     if constexpr (kLSW) {
-      bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * PP, xb[0], bar);
-      bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 4 * P, xb[1], bar);
-      if (xb[2]) bulk_g2s(sl + pl.oX[2], a.fld[2] + (size_t)e * PP, xb[2], bar);
+      bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * PP, nl * xb[0], bar);
+      bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 4 * P, nl * xb[1], bar);
+      if (xb[2]) bulk_g2s(sl + pl.oX[2], a.fld[2] + (size_t)e * PP, nl * xb[2], bar);
     } else if constexpr (kSW) {
-      if (xb[0]) bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * 4 * P, xb[0], bar);
-      if (xb[1]) bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 2 * PP, xb[1], bar);
+      if (xb[0]) bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * 4 * P, nl * xb[0], bar);
+      if (xb[1]) bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 2 * PP, nl * xb[1], bar);
     } else {
-      if (xb[0]) bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * 4 * PP, xb[0], bar);
-      if (xb[1]) bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 2 * PP + PP, xb[1], bar);
+      // environmentalsGradient (2,P,P,2,nEl): variable 1, both components, of each element
+      if (xb[0])
+        for (uint32_t x = 0; x < nl; ++x)
+          bulk_g2s(sl + pl.oX[0] + x * xb[0], a.fld[0] + (size_t)(e + x) * 4 * PP, xb[0], bar);
+      // environmentals (P,P,2,nEl): variable 2 (drag) of each element
+      if (xb[1])
+        for (uint32_t x = 0; x < nl; ++x)
+          bulk_g2s(sl + pl.oX[1] + x * xb[1], a.fld[1] + (size_t)(e + x) * 2 * PP + PP, xb[1], bar);
       if (xb[2])
-        for (int x = 2; x < 5; ++x) bulk_g2s(sl + pl.oX[x], a.fld[x] + (size_t)e * 16 * P, xb[x], bar);
+        for (int x = 2; x < 5; ++x) bulk_g2s(sl + pl.oX[x], a.fld[x] + (size_t)e * 16 * P, nl * xb[x], bar);
     }
   };
   if (t == 0) {
@@ -232,21 +262,31 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   }
 
   const int barId = 1 + g;
-  const bool active = t < PP;
-  const int i = t % P, j = t / P;
-  // Which warp of the group runs the face phase (the other one sums the
-  // divergence meanwhile): alternated in pairs of groups so that both kinds
-  // of work spread over the SM's four schedulers (warp w runs on w mod 4).
-  const int faceWarp = (TPE >= 64) ? ((g >> 1) & 1) : 0;
-  R* gU = reinterpret_cast<R*>(smem + pl.oGroups + (size_t)g * pl.groupBytes);  // fluxes, later node fields
-  R* gF1 = gU + NV * PP;                                                          // eta flux [NV][P][P]
-  R* gfb = gU + T::kU;                                                            // [4][SS]: [NV][P] per side
+  // node phases: thread t serves node n of element ee of the tile
+  const int ee = t / PP;
+  const int n = t - ee * PP;
+  const int i = n % P, j = n / P;
+  // Which warp of a one-element group runs the face phase (the other one sums
+  // the divergence meanwhile): alternated in pairs of groups so that both
+  // kinds of work spread over the SM's four schedulers (warp w runs on w mod
+  // 4).  Two-element groups give the divergence blocks to their first
+  // threads and the face nodes to their last ones.
+  const int faceWarp = (EPG == 1 && TPE >= 64) ? ((g >> 1) & 1) : 0;
+  R* gBase = reinterpret_cast<R*>(smem + pl.oGroups + (size_t)g * pl.groupBytes);
+  R* gU = gBase + ee * EB;      // this thread's element: fluxes, later node fields
+  R* gF1 = gU + NV * PP;        // eta flux [NV][P][P]
+  R* gfb = gU + T::kU;          // [4][SS]: [NV][P] per side
+  R* gD = (EPG > 1) ? gBase + EPG * EB + ee * NV * PP : gU;  // divergence sums
   R* trOut = reinterpret_cast<R*>(a.trOut);
+  constexpr int rNhat = 4 * PP * 8, rNs = rNhat + 8 * P * 8, rJ = rNs + 4 * P * 8, rSi = rJ + PP * 8;
 
   for (long long jj = 0;; ++jj) {
     const long long k = g + jj * C;
     if (k >= nMine) break;
-    const long long e = blockIdx.x + k * gridDim.x;
+    const long long e0 = (blockIdx.x + k * gridDim.x) * EPG;
+    const int nLive = (EPG == 1) ? 1 : tile_live(k);
+    const long long e = e0 + ee;
+    const bool active = (t < EPG * PP) && (ee < nLive);
     const int buf = (int)(jj & 1);
     const uint32_t par = (uint32_t)((jj >> 1) & 1);
     const unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
@@ -262,27 +302,27 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       }
       break;
     }
-    const int* ssi = reinterpret_cast<const int*>(sl + pl.oSi);
-    const double* sq = reinterpret_cast<const double*>(sl + pl.oQ);
+    const unsigned char* rec = sl + pl.oDsdx + (size_t)ee * gb;  // this thread's element's geometry record
+    const double* sq = reinterpret_cast<const double*>(sl + pl.oQ + (size_t)ee * qb);
     // node auxiliaries of this element, read from the buffer where they are used
     auto node_aux = [&](double na[3]) {
       na[0] = na[1] = na[2] = 0.0;
       if constexpr (kLSW) {
-        na[0] = reinterpret_cast<const double*>(sl + pl.oX[0])[t];
-        if (pl.oX[2] >= 0) na[1] = reinterpret_cast<const double*>(sl + pl.oX[2])[t];
+        na[0] = reinterpret_cast<const double*>(sl + pl.oX[0] + ee * xb[0])[n];
+        if (pl.oX[2] >= 0) na[1] = reinterpret_cast<const double*>(sl + pl.oX[2] + ee * xb[2])[n];
       } else if constexpr (kSW) {
         if (pl.oX[1] >= 0) {
-          const double* gg = reinterpret_cast<const double*>(sl + pl.oX[1]);
-          na[0] = gg[2 * t];
-          na[1] = gg[2 * t + 1];
+          const double* gg = reinterpret_cast<const double*>(sl + pl.oX[1] + ee * xb[1]);
+          na[0] = gg[2 * n];
+          na[1] = gg[2 * n + 1];
         }
       } else {
         if (pl.oX[0] >= 0) {
-          const double* gg = reinterpret_cast<const double*>(sl + pl.oX[0]);
-          na[0] = gg[2 * t];
-          na[1] = gg[2 * t + 1];
+          const double* gg = reinterpret_cast<const double*>(sl + pl.oX[0] + ee * xb[0]);
+          na[0] = gg[2 * n];
+          na[1] = gg[2 * n + 1];
         }
-        if (pl.oX[1] >= 0) na[2] = reinterpret_cast<const double*>(sl + pl.oX[1])[t];
+        if (pl.oX[1] >= 0) na[2] = reinterpret_cast<const double*>(sl + pl.oX[1] + ee * xb[1])[n];
       }
     };
 
@@ -293,15 +333,15 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     R f[NF];
     if (active) {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) f[v] = (R)sq[t + PP * v];
+      for (int v = 0; v < NV; ++v) f[v] = (R)sq[n + PP * v];
       Phys::template node_flux<R>(f, a);
       double na[3];
       node_aux(na);
       R Fx[NV], Fy[NV];
       Phys::template flux<R>(f, na, a, Fx, Fy);
       // dsdx planes: (dsdx11, dsdx21) of every node, then (dsdx12, dsdx22)
-      const double2* gp = reinterpret_cast<const double2*>(sl + pl.oDsdx);
-      const double2 c1 = gp[t], c2 = gp[PP + t];
+      const double2* gp = reinterpret_cast<const double2*>(rec);
+      const double2 c1 = gp[n], c2 = gp[PP + n];
       R F0[NV], F1[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
@@ -309,147 +349,167 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         F1[v] = (R)c2.x * Fx[v] + (R)c2.y * Fy[v];
       }
       if constexpr (NV == 4)
-        if (a.av) av_volume_add<P, R>(a, t, e, F0, F1);
+        if (a.av) av_volume_add<P, R>(a, n, e, F0, F1);
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
         gU[v * PP + P * j + T::f0pos(i, j)] = F0[v];
-        gF1[v * PP + t] = F1[v];
+        gF1[v * PP + n] = F1[v];
       }
     }
     named_bar(barId, TPE);  // contravariant fluxes ready
 
-    // ---- B (alongside the face phase C, in the group's other warp): weak-
-    // divergence volume sums, the reference's order per node and variable
-    // (VectorDGDivergence_2D, src/SELF_Lagrange.f90):
+    // ---- B (alongside the face phase C): weak-divergence volume sums, the
+    // reference's order per node and variable (VectorDGDivergence_2D,
+    // src/SELF_Lagrange.f90):
     //   d = 0;  for m ascending: d = (d + dgM(m,i) F0(m,j)) + dgM(m,j) F1(i,m).
     // A thread sums a 2x2 block of nodes for two variables, so every loaded
-    // flux pair and dgMatrix pair serves two nodes.  The sums replace the xi
-    // flux in shared memory ([NV][P^2], node-major) once the warp has read it.
-    if (TPE < 64 || (t >> 5) != faceWarp) {
-      using R2 = typename std::conditional<sizeof(R) == 8, double2, float2>::type;
-      constexpr int HB = T::HB;
-      const int tb = t & 31;
-      const bool on = tb < T::NB;
-      const int vp = tb / (HB * HB), rem = tb - vp * (HB * HB), bj = rem / HB, bi = rem - bj * HB;
-      const int v0 = 2 * vp;
-      const bool two = v0 + 1 < NV;
-      R acc[2][2][2];  // [variable of the pair][row offset r (j)][column offset c (i)]
-#pragma unroll
-      for (int vv = 0; vv < 2; ++vv)
-#pragma unroll
-        for (int r = 0; r < 2; ++r) acc[vv][r][0] = acc[vv][r][1] = (R)0;
-      if (on) {
-        const double2* sdg2 = reinterpret_cast<const double2*>(sdg);
-#pragma unroll
-        for (int mp = 0; mp < HB; ++mp) {
-          R f0[2][2][2];  // [vv][r][k]: F0(2 mp + k, 2 bj + r)
-          R f1[2][2][2];  // [vv][k][c]: F1(2 bi + c, 2 mp + k)
-#pragma unroll
-          for (int vv = 0; vv < 2; ++vv) {
-            const int v = (vv == 0 || two) ? v0 + vv : v0;
-#pragma unroll
-            for (int r = 0; r < 2; ++r) {
-              const int row = 2 * bj + r;
-              const R2 x = reinterpret_cast<const R2*>(gU + v * PP + P * row)[T::f0pos(2 * mp, row) >> 1];
-              f0[vv][r][0] = x.x;
-              f0[vv][r][1] = x.y;
-            }
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-              const R2 x = reinterpret_cast<const R2*>(gF1 + v * PP + P * (2 * mp + k))[bi];
-              f1[vv][k][0] = x.x;
-              f1[vv][k][1] = x.y;
-            }
-          }
-#pragma unroll
-          for (int k = 0; k < 2; ++k) {
-            const int m = 2 * mp + k;
-            const double2 dI = sdg2[bi + HB * m], dJ = sdg2[bj + HB * m];
-            const R gi[2] = {(R)dI.x, (R)dI.y}, gj[2] = {(R)dJ.x, (R)dJ.y};
-#pragma unroll
-            for (int vv = 0; vv < 2; ++vv)
-#pragma unroll
-              for (int r = 0; r < 2; ++r)
-#pragma unroll
-                for (int c = 0; c < 2; ++c)
-                  acc[vv][r][c] = acc[vv][r][c] + gi[c] * f0[vv][r][k] + gj[r] * f1[vv][k][c];
-          }
-        }
-      }
-      __syncwarp();  // the warp has read the xi flux
-      if (on) {
+    // flux pair and dgMatrix pair serves two nodes.  One-element groups write
+    // the sums over the xi flux ([NV][P^2], node-major) once the warp has read
+    // it; two-element groups write them to their separate array.
+    {
+      const bool mine = (EPG == 1) ? (TPE < 64 || (t >> 5) != faceWarp) : (t < EPG * T::NB);
+      if (mine) {
+        using R2 = typename std::conditional<sizeof(R) == 8, double2, float2>::type;
+        constexpr int HB = T::HB;
+        const int eB = (EPG == 1) ? 0 : t / T::NB;
+        const int tb = (EPG == 1) ? (t & 31) : t - eB * T::NB;
+        const bool on = (EPG == 1) ? (tb < T::NB) : (eB < nLive);
+        const R* bU = gBase + eB * EB;
+        const R* bF1 = bU + NV * PP;
+        R* bD = (EPG > 1) ? gBase + EPG * EB + eB * NV * PP : gBase;
+        const int vp = tb / (HB * HB), rem = tb - vp * (HB * HB), bj = rem / HB, bi = rem - bj * HB;
+        const int v0 = 2 * vp;
+        const bool two = v0 + 1 < NV;
+        R acc[2][2][2];  // [variable of the pair][row offset r (j)][column offset c (i)]
 #pragma unroll
         for (int vv = 0; vv < 2; ++vv)
-          if (vv == 0 || two)
 #pragma unroll
-            for (int r = 0; r < 2; ++r) {
-              R2 x;
-              x.x = acc[vv][r][0];
-              x.y = acc[vv][r][1];
-              reinterpret_cast<R2*>(gU + (v0 + vv) * PP + P * (2 * bj + r))[bi] = x;
+          for (int r = 0; r < 2; ++r) acc[vv][r][0] = acc[vv][r][1] = (R)0;
+        if (on) {
+          const double2* sdg2 = reinterpret_cast<const double2*>(sdg);
+#pragma unroll
+          for (int mp = 0; mp < HB; ++mp) {
+            R f0[2][2][2];  // [vv][r][k]: F0(2 mp + k, 2 bj + r)
+            R f1[2][2][2];  // [vv][k][c]: F1(2 bi + c, 2 mp + k)
+#pragma unroll
+            for (int vv = 0; vv < 2; ++vv) {
+              const int v = (vv == 0 || two) ? v0 + vv : v0;
+#pragma unroll
+              for (int r = 0; r < 2; ++r) {
+                const int row = 2 * bj + r;
+                const R2 x = reinterpret_cast<const R2*>(bU + v * PP + P * row)[T::f0pos(2 * mp, row) >> 1];
+                f0[vv][r][0] = x.x;
+                f0[vv][r][1] = x.y;
+              }
+#pragma unroll
+              for (int kq = 0; kq < 2; ++kq) {
+                const R2 x = reinterpret_cast<const R2*>(bF1 + v * PP + P * (2 * mp + kq))[bi];
+                f1[vv][kq][0] = x.x;
+                f1[vv][kq][1] = x.y;
+              }
             }
+#pragma unroll
+            for (int kq = 0; kq < 2; ++kq) {
+              const int m = 2 * mp + kq;
+              const double2 dI = sdg2[bi + HB * m], dJ = sdg2[bj + HB * m];
+              const R gi[2] = {(R)dI.x, (R)dI.y}, gj[2] = {(R)dJ.x, (R)dJ.y};
+#pragma unroll
+              for (int vv = 0; vv < 2; ++vv)
+#pragma unroll
+                for (int r = 0; r < 2; ++r)
+#pragma unroll
+                  for (int c = 0; c < 2; ++c)
+                    acc[vv][r][c] = acc[vv][r][c] + gi[c] * f0[vv][r][kq] + gj[r] * f1[vv][kq][c];
+            }
+          }
+        }
+        if constexpr (EPG == 1) __syncwarp();  // the warp has read the xi flux it overwrites
+        if (on) {
+#pragma unroll
+          for (int vv = 0; vv < 2; ++vv)
+            if (vv == 0 || two)
+#pragma unroll
+              for (int r = 0; r < 2; ++r) {
+                R2 x;
+                x.x = acc[vv][r][0];
+                x.y = acc[vv][r][1];
+                reinterpret_cast<R2*>(bD + (v0 + vv) * PP + P * (2 * bj + r))[bi] = x;
+              }
+        }
       }
     }
 
     // ---- C: faces; own traces of this stage's solution come from the cache
-    if ((t >> 5) == faceWarp && (t & 31) < 4 * P) {
-      const int s1 = (t & 31) / P, ii = (t & 31) % P;
-      const int bcid = ssi[5 * s1 + 4];
-      const bool physical = (bcid != 0) && (ssi[5 * s1 + 2] == 0);
-      const int flip = ssi[5 * s1 + 3] % 10;
-      const R* own = reinterpret_cast<const R*>(sl + pl.oOwn) + s1 * TS;
-      const int i2 = flip ? N - ii : ii;
-      const long long nb = (bcid == 0) ? (long long)TS * (ssi[5 * s1 + 3] / 10 - 1 + 4 * (long long)(ssi[5 * s1 + 2] - 1))
-                                       : -1;
-      const R* nbr = reinterpret_cast<const R*>(a.trIn) + (nb < 0 ? 0 : nb);
-      R L[NT], X[NT];
+    {
+      const int c0 = TPE - EPG * 4 * P;  // first face thread of a two-element group
+      const bool mine = (EPG == 1) ? ((t >> 5) == faceWarp && (t & 31) < 4 * P) : (t >= c0);
+      const int cf = (EPG == 1) ? (t & 31) : t - c0;
+      const int eC = cf / (4 * P);
+      if (mine && eC < nLive) {
+        const int cc = cf - eC * 4 * P;
+        const int s1 = cc / P, ii = cc % P;
+        const long long eF = e0 + eC;
+        const unsigned char* recC = sl + pl.oDsdx + (size_t)eC * gb;
+        const int* ssi = reinterpret_cast<const int*>(recC + rSi);
+        const int bcid = ssi[5 * s1 + 4];
+        const bool physical = (bcid != 0) && (ssi[5 * s1 + 2] == 0);
+        const int flip = ssi[5 * s1 + 3] % 10;
+        const R* own = reinterpret_cast<const R*>(sl + pl.oOwn + (size_t)eC * ob) + s1 * TS;
+        const int i2 = flip ? N - ii : ii;
+        const long long nb =
+            (bcid == 0) ? (long long)TS * (ssi[5 * s1 + 3] / 10 - 1 + 4 * (long long)(ssi[5 * s1 + 2] - 1)) : -1;
+        const R* nbr = reinterpret_cast<const R*>(a.trIn) + (nb < 0 ? 0 : nb);
+        R L[NT], X[NT];
 #pragma unroll
-      for (int kf = 0; kf < NT; ++kf) {
-        L[kf] = own[ii + P * kf];
-        X[kf] = (nb >= 0) ? nbr[i2 + P * kf] : (R)0;
-      }
-      const double2 nh = reinterpret_cast<const double2*>(sl + pl.oNhat)[ii + P * s1];
-      const double ns = reinterpret_cast<const double*>(sl + pl.oNs)[ii + P * s1];
-      double fx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-      if constexpr (kLSW) {
-        fx[0] = reinterpret_cast<const double*>(sl + pl.oX[1])[ii + P * s1];
-      } else if constexpr (kSW) {
-        if (physical && pl.oX[0] >= 0) fx[0] = reinterpret_cast<const double*>(sl + pl.oX[0])[ii + P * s1];
-      } else {
-        if (physical && pl.oX[2] >= 0) {
-          const double* ps = reinterpret_cast<const double*>(sl + pl.oX[2]);
-          const double* pp = reinterpret_cast<const double*>(sl + pl.oX[3]);
-          const double* pd = reinterpret_cast<const double*>(sl + pl.oX[4]);
-          const int b = ii + P * 4 * s1;
-          for (int v = 0; v < 4; ++v) fx[v] = ps[b + v * P];
-          fx[4] = pp[b];
-          fx[5] = pp[b + P];
-          fx[6] = pp[b + 3 * P];
-          fx[7] = pd[b + P];
-          fx[8] = pd[b + 2 * P];
+        for (int kf = 0; kf < NT; ++kf) {
+          L[kf] = own[ii + P * kf];
+          X[kf] = (nb >= 0) ? nbr[i2 + P * kf] : (R)0;
         }
-      }
-      R velL[2] = {(R)0, (R)0}, velR[2] = {(R)0, (R)0};
-      if constexpr (kSW) {
-        const R* vo = reinterpret_cast<const R*>(sl + pl.oVelOwn);
-        velL[0] = vo[ii + P * (0 + 2 * s1)];
-        velL[1] = vo[ii + P * (1 + 2 * s1)];
-        if (nb >= 0) {  // the neighbour's stage-lagged velocity traces, plain loads
-          const R* vn = reinterpret_cast<const R*>(a.velIn) +
-                        (size_t)2 * P * (ssi[5 * s1 + 3] / 10 - 1 + 4 * (size_t)(ssi[5 * s1 + 2] - 1));
-          velR[0] = vn[i2];
-          velR[1] = vn[i2 + P];
+        const double2 nh = reinterpret_cast<const double2*>(recC + rNhat)[ii + P * s1];
+        const double ns = reinterpret_cast<const double*>(recC + rNs)[ii + P * s1];
+        double fx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if constexpr (kLSW) {
+          fx[0] = reinterpret_cast<const double*>(sl + pl.oX[1] + eC * xb[1])[ii + P * s1];
+        } else if constexpr (kSW) {
+          if (physical && pl.oX[0] >= 0)
+            fx[0] = reinterpret_cast<const double*>(sl + pl.oX[0] + eC * xb[0])[ii + P * s1];
+        } else {
+          if (physical && pl.oX[2] >= 0) {
+            const double* ps = reinterpret_cast<const double*>(sl + pl.oX[2] + eC * xb[2]);
+            const double* pp = reinterpret_cast<const double*>(sl + pl.oX[3] + eC * xb[3]);
+            const double* pd = reinterpret_cast<const double*>(sl + pl.oX[4] + eC * xb[4]);
+            const int b = ii + P * 4 * s1;
+            for (int v = 0; v < 4; ++v) fx[v] = ps[b + v * P];
+            fx[4] = pp[b];
+            fx[5] = pp[b + P];
+            fx[6] = pp[b + 3 * P];
+            fx[7] = pd[b + P];
+            fx[8] = pd[b + 2 * P];
+          }
         }
-        R* vOut = reinterpret_cast<R*>(a.velOut);
-        vOut[ii + P * (0 + 2 * (s1 + 4 * e))] = L[0] / L[2];
-        vOut[ii + P * (1 + 2 * (s1 + 4 * e))] = L[1] / L[2];
-      }
-      R out[NV];
-      Phys::template face<R>(bcid, physical, L, X, velL, velR, nh.x, nh.y, ns, fx, a, out);
-      if constexpr (NV == 4)
-        if (a.av) av_face_add<P, R>(a, s1, ii, e, ssi + 5 * s1, nh.x, nh.y, ns, out);
+        R velL[2] = {(R)0, (R)0}, velR[2] = {(R)0, (R)0};
+        if constexpr (kSW) {
+          const R* vo = reinterpret_cast<const R*>(sl + pl.oVelOwn + (size_t)eC * vb);
+          velL[0] = vo[ii + P * (0 + 2 * s1)];
+          velL[1] = vo[ii + P * (1 + 2 * s1)];
+          if (nb >= 0) {  // the neighbour's stage-lagged velocity traces, plain loads
+            const R* vn = reinterpret_cast<const R*>(a.velIn) +
+                          (size_t)2 * P * (ssi[5 * s1 + 3] / 10 - 1 + 4 * (size_t)(ssi[5 * s1 + 2] - 1));
+            velR[0] = vn[i2];
+            velR[1] = vn[i2 + P];
+          }
+          R* vOut = reinterpret_cast<R*>(a.velOut);
+          vOut[ii + P * (0 + 2 * (s1 + 4 * eF))] = L[0] / L[2];
+          vOut[ii + P * (1 + 2 * (s1 + 4 * eF))] = L[1] / L[2];
+        }
+        R out[NV];
+        Phys::template face<R>(bcid, physical, L, X, velL, velR, nh.x, nh.y, ns, fx, a, out);
+        if constexpr (NV == 4)
+          if (a.av) av_face_add<P, R>(a, s1, ii, eF, ssi + 5 * s1, nh.x, nh.y, ns, out);
+        R* fb = gBase + eC * EB + T::kU;
 #pragma unroll
-      for (int v = 0; v < NV; ++v) gfb[s1 * SS + v * P + ii] = out[v];
+        for (int v = 0; v < NV; ++v) fb[s1 * SS + v * P + ii] = out[v];
+      }
     }
     named_bar(barId, TPE);  // flux and face values ready
 
@@ -458,19 +518,19 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     if (active) {
       if (rk) {  // RK register from global memory; the lift below hides the latency
 #pragma unroll
-        for (int v = 0; v < NV; ++v) Gv[v] = a.G[t + (size_t)PP * (v + NV * (size_t)e)];
+        for (int v = 0; v < NV; ++v) Gv[v] = a.G[n + (size_t)PP * (v + NV * (size_t)e)];
       }
 #pragma unroll
-      for (int v = 0; v < NV; ++v) qv[v] = sq[t + PP * v];
+      for (int v = 0; v < NV; ++v) qv[v] = sq[n + PP * v];
       // J of the node (reference-rounding build) or 1/J (the other forms)
-      const double Jij = reinterpret_cast<const double*>(sl + pl.oJ)[t];
+      const double Jij = reinterpret_cast<const double*>(rec + rJ)[n];
       // sources in FP64 in every form (well-balanced topography / gravity terms)
       double Src[NV], na[3];
       node_aux(na);
       Phys::template source<double>(qv, na, a, Src);
       R d[NV];  // volume sums from phase B
 #pragma unroll
-      for (int v = 0; v < NV; ++v) d[v] = gU[v * PP + t];
+      for (int v = 0; v < NV; ++v) d[v] = gD[v * PP + n];
       if constexpr (ref_rounding<R>()) {
         // the reference's divisions, rounded as it rounds them (bit-exact form)
         const R wi = (R)sqw[i], wj = (R)sqw[j];
@@ -493,7 +553,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         }
       }
     }
-    named_bar(barId, TPE);  // every thread is done reading the flux array and the buffer
+    named_bar(barId, TPE);  // every thread is done reading the flux arrays and the buffer
     if (t == 0) {  // refill the buffer: generic-proxy reads before the async-proxy writes
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       issue(jj + 2);
@@ -501,14 +561,14 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     if (!rk) {
       if (active)
 #pragma unroll
-        for (int v = 0; v < NV; ++v) a.dSdt[t + (size_t)PP * (v + NV * (size_t)e)] = dsdt[v];
+        for (int v = 0; v < NV; ++v) a.dSdt[n + (size_t)PP * (v + NV * (size_t)e)] = dsdt[v];
       continue;
     }
     if (active) {
       const double gdt = a.dtElem ? a.rk_g * a.dtElem[e] : a.rk_gdt;
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        const size_t gi = t + (size_t)PP * (v + NV * (size_t)e);
+        const size_t gi = n + (size_t)PP * (v + NV * (size_t)e);
         const double Gn = a.rk_a * Gv[v] + dsdt[v];
         a.G[gi] = Gn;
         const double qn = qv[v] + gdt * Gn;
@@ -522,21 +582,25 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     named_bar(barId, TPE);
 
     // ---- E: traces of the updated solution -> trace cache.  One task per
-    // (field, line, orientation) reads the line's P values once and forms both
-    // of its end traces (BoundaryInterp, src/SELF_Lagrange.f90:2241-2270):
-    // column l gives S (side 0) and N (side 2), row l gives W (3) and E (1).
-    // Tasks are numbered by field pair, orientation, field, line, so that for
-    // P = 8 a half-warp reads the column lines (or the row lines) of two fields.
+    // (element, field, line, orientation) reads the line's P values once and
+    // forms both of its end traces (BoundaryInterp, src/SELF_Lagrange.f90:
+    // 2241-2270): column l gives S (side 0) and N (side 2), row l gives W (3)
+    // and E (1).  Tasks are numbered by field pair, orientation, field, line,
+    // so that for P = 8 a half-warp reads the column lines (or the row lines)
+    // of two fields.
     {
-      R* o = trOut + (size_t)4 * TS * e;
       constexpr int NTp = (NT + 1) / 2 * 2;
-      // the face warp starts one warp later, so the other warp takes the
-      // last, partial round
-      for (int kk = faceWarp ? t : (t + 32) % TPE; kk < 2 * NTp * P; kk += TPE) {
-        const int fp = kk / (4 * P), r = kk - fp * 4 * P, row = r / (2 * P), r2 = r - row * 2 * P, fs = r2 / P;
+      constexpr int TPEl = 2 * NTp * P;  // tasks per element
+      // a one-element group's face warp starts one warp later, so the other
+      // warp takes the last, partial round
+      const int k0 = (EPG == 1) ? (faceWarp ? t : (t + 32) % TPE) : t;
+      for (int kk = k0; kk < EPG * TPEl; kk += TPE) {
+        const int eE = kk / TPEl, ks = kk - eE * TPEl;
+        if (eE >= nLive) continue;
+        const int fp = ks / (4 * P), r = ks - fp * 4 * P, row = r / (2 * P), r2 = r - row * 2 * P, fs = r2 / P;
         const int l = r2 - fs * P, fi = 2 * fp + fs;
         if (fi >= NT) continue;
-        const R* fv = gU + fi * FS;
+        const R* fv = gBase + eE * EB + fi * FS;
         R lo = (R)0, hi = (R)0;
 #pragma unroll
         for (int m = 0; m < P; ++m) {
@@ -544,11 +608,12 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
           lo = lo + bm_left<R>(a, m) * x;
           hi = hi + bm_right<R, P>(a, m) * x;
         }
+        R* o = trOut + (size_t)4 * TS * (e0 + eE);
         o[l + P * fi + TS * (row ? 3 : 0)] = lo;
         o[l + P * fi + TS * (row ? 1 : 2)] = hi;
       }
     }
-    // no barrier here: the next element's post-wait barrier orders the reuse of gU
+    // no barrier here: the next tile's post-wait barrier orders the reuse of the arrays
   }
 }
 
@@ -556,20 +621,20 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
 template <int P, class Phys, typename R>
 inline bool make_tma_plan(const StageArgs& a, int smemLimit, TmaPlan& pl, int maxGroups = 0) {
   using T = TmaTraits<P, Phys, R>;
-  constexpr int PP = T::PP, NV = T::NV, TS = T::TS;
+  constexpr int PP = T::PP, NV = T::NV, TS = T::TS, EPG = T::EPG;
   constexpr bool kLSW = (NV == 3 && !Phys::kLaggedVelocity);
   constexpr bool kSW = Phys::kLaggedVelocity;
   if (P % 2 != 0) return false;
   int o = 0;
-  auto put = [&](int bytes) {
+  auto put = [&](int bytes) {  // one piece of a tile: EPG elements' blocks back to back
     int at = o;
-    o += (bytes + 15) / 16 * 16;
+    o += (EPG * bytes + 15) / 16 * 16;
     return at;
   };
   if (!a.geo) return false;
   pl.oQ = put(NV * PP * 8);
-  pl.oDsdx = put(geo_record_doubles<P>() * 8);  // packed record: dsdx, nHat, nScale, J, sideInfo
-  pl.oNhat = pl.oDsdx + 4 * PP * 8;
+  pl.oDsdx = put(geo_record_doubles<P>() * 8);  // packed records: dsdx, nHat, nScale, J, sideInfo
+  pl.oNhat = pl.oDsdx + 4 * PP * 8;              // (offsets within the first element's record)
   pl.oNs = pl.oNhat + 8 * P * 8;
   pl.oJ = pl.oNs + 4 * P * 8;
   pl.oSi = pl.oJ + PP * 8;

@@ -49,7 +49,8 @@ cudaError_t launch_one(const StageArgs& a, const StageLaunch& L, cudaStream_t st
         attrSet.fetch_or(bit);
       }
       using T = TmaTraits<P, Phys, R>;
-      const int grid = a.nEl < L.numSMs ? a.nEl : L.numSMs;
+      const int tiles = (a.nEl + T::EPG - 1) / T::EPG;  // work items of EPG consecutive elements
+      const int grid = tiles < L.numSMs ? tiles : L.numSMs;
       // Programmatic dependent launch: the launch and the kernel's prologue
       // overlap the end of the previous kernel on the stream; the kernel waits
       // for that kernel's completion (griddepcontrol.wait) before it touches
