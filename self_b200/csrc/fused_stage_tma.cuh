@@ -88,18 +88,20 @@ template <int P, class Phys, typename R>
 struct TmaTraits {
   static constexpr int PP = P * P, NV = Phys::NV, NT = Phys::NT, NF = Phys::NF;
   static constexpr int TS = trace_side_stride<P, NT, R>();
-  // Elements per group: a P = 4 element (16 nodes) would leave half of its
-  // warp's lanes idle, so its groups take two elements at a time (a tile of
-  // consecutive elements).  P = 6 stays at one element per two-warp group:
-  // two elements in three warps measured slower (six groups at 96 registers
-  // with spills against ten groups).  The code serves any EPG.
-  static constexpr int EPG = (P == 4) ? 2 : 1;
+  // Elements per group (a tile of consecutive elements).  A P = 4 element
+  // (16 nodes) would leave half of its warp's lanes idle: two per one-warp
+  // group.  A P = 6 element (36 nodes) on a two-warp group leaves 28 lanes
+  // idle: four per five-warp group (144 of 160 lanes), measured 1.14x faster
+  // for ShallowWater FP64 and 1.12x for CompressibleIdealGas2D FP32, but
+  // 1.17x slower for CompressibleIdealGas2D FP64, whose larger tiles leave
+  // room for three groups only; that case keeps one element per group.
+  static constexpr int EPG = (P == 4) ? 2 : ((P == 6 && !(NV == 4 && sizeof(R) == 8)) ? 4 : 1);
   static constexpr int TPE = (EPG * PP + 31) / 32 * 32;  // threads per group
   static_assert(TPE >= EPG * 4 * P, "the face phase gives each of the 4P face nodes its own thread");
-  // 640 threads (five warps per scheduler at 96 registers) for P = 6 and 8,
-  // up to 15 single-warp groups for P <= 4 (named barriers 1..15; barrier 0
-  // is the CTA-wide one)
-  static constexpr int kMaxGroups = (P <= 4) ? 15 : (P == 6 && EPG == 2 ? 6 : 10);
+  // 640 threads (five warps per scheduler at 96 registers) for P = 6 (ten
+  // one-element or four four-element groups) and P = 8, up to 15 single-warp
+  // groups for P <= 4 (named barriers 1..15; barrier 0 is the CTA-wide one)
+  static constexpr int kMaxGroups = (P <= 4) ? 15 : (P == 6 ? 640 / TPE : 10);
   static constexpr int kThreadsMax = kMaxGroups * TPE;
   // Per-element compute arrays (bulk type), laid out for conflict-free shared
   // accesses.  A 64-bit shared access is served per half-warp: two threads of
