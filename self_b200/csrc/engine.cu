@@ -552,16 +552,18 @@ int selfgpu_model2d_rk3(selfgpu_model2d* m, double dt, int nSteps) {
   if (rc) return rc;
   if (nSteps < 0) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_rk3: nSteps < 0");
   cudaError_t e = cudaSuccess;
-  if (!m->valid) {
-    e = m->prologue();
-    if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_rk3", e);
-  }
   if (m->multistep && nSteps > 0 && m->avMode == AV_OFF && m->nHalo == 0 && !m->base.debugStarve) {
+    e = m->valid ? cudaSuccess : m->prologue();
+    if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_rk3", e);
     e = m->launch_steps(dt, nSteps);
     if (e == cudaSuccess) return SELFGPU_OK;
     cudaGetLastError();
     if (e != cudaErrorCooperativeLaunchTooLarge) return fail_cuda("selfgpu_model2d_rk3: multi-step launch", e);
     // the mesh does not fit one wave: graph-replayed steps below
+  }
+  if (!m->valid) {
+    e = m->prologue();
+    if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_rk3", e);
   }
   if (!(dt == m->graphDt)) m->drop_graphs();
   for (int s = 0; s < nSteps; ++s) {

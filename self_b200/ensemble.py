@@ -103,17 +103,18 @@ class _Ensemble:
     """Instances grouped by degree; one fused handle per degree on its own
     stream.  Subclasses build a group's model (_build_group)."""
 
-    def __init__(self, instances, form, autotune):
+    def __init__(self, instances, form, autotune, shared_stream=False):
         self.instances, self.form = instances, form
         self.groups = {}
         for inst in instances:
             self.groups.setdefault(inst.N, []).append(inst)
         self.handles = {}
+        one = torch.cuda.Stream() if shared_stream else None
         for gi, (N, members) in enumerate(sorted(self.groups.items())):
             mesh, offs = concat_meshes([self._instance_mesh(i) for i in members])
             for inst, off in zip(members, offs):
                 inst.offset, inst.group = off, gi
-            stream = torch.cuda.Stream()
+            stream = one if one is not None else torch.cuda.Stream()
             h = self._build_group(N, members, mesh, stream)
             h.update(stream=stream, mesh=mesh, members=members)
             h["q0"] = h["model"].solution.clone()
@@ -155,9 +156,9 @@ class _Ensemble:
 class ShallowWaterEnsemble(_Ensemble):
     """Batched ShallowWater instances."""
 
-    def __init__(self, instances, form=A.FP32_BULK, cfl=0.5, autotune=True, g=1.0):
+    def __init__(self, instances, form=A.FP32_BULK, cfl=0.5, autotune=True, g=1.0, shared_stream=False):
         self.cfl, self.g = cfl, g
-        super().__init__(instances, form, autotune)
+        super().__init__(instances, form, autotune, shared_stream)
 
     @staticmethod
     def _instance_mesh(inst):
