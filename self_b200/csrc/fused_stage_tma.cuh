@@ -368,7 +368,45 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     // flux pair and dgMatrix pair serves two nodes.  One-element groups write
     // the sums over the xi flux ([NV][P^2], node-major) once the warp has read
     // it; two-element groups write them to their separate array.
-    {
+    // Production FP64 form at P = 8: the same sums as FP64 tensor-core
+    // products (mma.sync m8n8k4 f64), D(j,i) = sum_m F0(m,j) dgM(m,i) +
+    // dgM(m,j) F1(i,m), four chained products per variable over the group's
+    // divergence warp; the order of the additions inside a product is the
+    // hardware's, so only the forms without the reference's rounding use it.
+    constexpr bool kDmma = (P == 8) && (EPG == 1) && (sizeof(R) == 8) && !ref_rounding<R>();
+    if constexpr (kDmma) {
+      if ((t >> 5) != faceWarp) {
+        const int lane = t & 31, gq = lane >> 2, kq = lane & 3;
+        double dv[NV][2];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          double c0 = 0.0, c1 = 0.0;
+#pragma unroll
+          for (int kk = 0; kk < 2; ++kk) {
+            const int m = 4 * kk + kq;
+            const double aF0 = (double)gU[v * PP + P * gq + T::f0pos(m, gq)];  // F0 at node (m, j = gq)
+            const double dg = sdg[gq + P * m];                               // dgM(m, gq)
+            const double bF1 = (double)gF1[v * PP + P * m + gq];             // F1 at node (i = gq, m)
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                         : "+d"(c0), "+d"(c1)
+                         : "d"(aF0), "d"(dg));
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                         : "+d"(c0), "+d"(c1)
+                         : "d"(dg), "d"(bF1));
+          }
+          dv[v][0] = c0;  // D(j = gq, i = 2 kq), D(gq, 2 kq + 1)
+          dv[v][1] = c1;
+        }
+        __syncwarp();  // the warp has read the xi flux it overwrites
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          double2 x;
+          x.x = dv[v][0];
+          x.y = dv[v][1];
+          reinterpret_cast<double2*>(gD + v * PP + P * gq)[kq] = x;
+        }
+      }
+    } else {
       const bool mine = (EPG == 1) ? (TPE < 64 || (t >> 5) != faceWarp) : (t < EPG * T::NB);
       if (mine) {
         using R2 = typename std::conditional<sizeof(R) == 8, double2, float2>::type;
