@@ -368,12 +368,14 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     // flux pair and dgMatrix pair serves two nodes.  One-element groups write
     // the sums over the xi flux ([NV][P^2], node-major) once the warp has read
     // it; two-element groups write them to their separate array.
-    // Production FP64 form at P = 8: the same sums as FP64 tensor-core
-    // products (mma.sync m8n8k4 f64), D(j,i) = sum_m F0(m,j) dgM(m,i) +
-    // dgM(m,j) F1(i,m), four chained products per variable over the group's
-    // divergence warp; the order of the additions inside a product is the
-    // hardware's, so only the forms without the reference's rounding use it.
-    constexpr bool kDmma = (P == 8) && (EPG == 1) && (sizeof(R) == 8) && !ref_rounding<R>();
+    // Production FP64 and FP32-bulk forms at P = 8: the same sums as FP64
+    // tensor-core products (mma.sync m8n8k4 f64), D(j,i) = sum_m F0(m,j)
+    // dgM(m,i) + dgM(m,j) F1(i,m), four chained products per variable over the
+    // group's divergence warp (FP32-bulk fluxes are widened exactly to FP64 and
+    // the sums rounded back once); the order of the additions inside a product
+    // is the hardware's, so only the forms without the reference's rounding
+    // use it.
+    constexpr bool kDmma = (P == 8) && (EPG == 1) && !ref_rounding<R>();
     if constexpr (kDmma) {
       if ((t >> 5) != faceWarp) {
         const int lane = t & 31, gq = lane >> 2, kq = lane & 3;
@@ -398,12 +400,13 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
           dv[v][1] = c1;
         }
         __syncwarp();  // the warp has read the xi flux it overwrites
+        using R2 = typename std::conditional<sizeof(R) == 8, double2, float2>::type;
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-          double2 x;
-          x.x = dv[v][0];
-          x.y = dv[v][1];
-          reinterpret_cast<double2*>(gD + v * PP + P * gq)[kq] = x;
+          R2 x;
+          x.x = (R)dv[v][0];
+          x.y = (R)dv[v][1];
+          reinterpret_cast<R2*>(gD + v * PP + P * gq)[kq] = x;
         }
       }
     } else {
