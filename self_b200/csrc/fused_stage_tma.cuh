@@ -368,16 +368,24 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     // flux pair and dgMatrix pair serves two nodes.  One-element groups write
     // the sums over the xi flux ([NV][P^2], node-major) once the warp has read
     // it; two-element groups write them to their separate array.
-    // Production FP64 and FP32-bulk forms at P = 8: the same sums as FP64
-    // tensor-core products (mma.sync m8n8k4 f64), D(j,i) = sum_m F0(m,j)
-    // dgM(m,i) + dgM(m,j) F1(i,m), four chained products per variable over the
-    // group's divergence warp (FP32-bulk fluxes are widened exactly to FP64 and
-    // the sums rounded back once); the order of the additions inside a product
-    // is the hardware's, so only the forms without the reference's rounding
-    // use it.
-    constexpr bool kDmma = (P == 8) && (EPG == 1) && !ref_rounding<R>();
+    // Production FP64 and FP32-bulk forms at P = 8 and P = 6: the same sums
+    // as FP64 tensor-core products (mma.sync m8n8k4 f64), D(j,i) = sum_m
+    // F0(m,j) dgM(m,i) + dgM(m,j) F1(i,m), four chained products per variable
+    // over one warp per element (a P = 6 element is padded with zeros to the
+    // 8x8 shape; FP32-bulk fluxes are widened exactly to FP64 and the sums
+    // rounded back once).  The order of the additions inside a product is the
+    // hardware's, so only the forms without the reference's rounding use it.
+    constexpr bool kDmma = ((P == 8 && EPG == 1) || P == 6) && !ref_rounding<R>();
     if constexpr (kDmma) {
-      if ((t >> 5) != faceWarp) {
+      // the warps a tile's face threads leave free take its elements in turn
+      // (a one-element group: the warp that is not the face warp)
+      constexpr int kDW = (EPG == 1) ? 1 : ((TPE - EPG * 4 * P) / 32 > 0 ? (TPE - EPG * 4 * P) / 32 : 1);
+      const int w = t >> 5;
+      const bool run = (EPG == 1) ? (w != faceWarp) : (w < kDW);
+      for (int eB = (EPG == 1) ? 0 : w; run && eB < nLive; eB += kDW) {  // uniform over the warp
+        const R* bU = gBase + eB * EB;
+        const R* bF1 = bU + NV * PP;
+        R* bD = (EPG > 1) ? gBase + EPG * EB + eB * NV * PP : gBase;
         const int lane = t & 31, gq = lane >> 2, kq = lane & 3;
         double dv[NV][2];
 #pragma unroll
@@ -386,27 +394,30 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
 #pragma unroll
           for (int kk = 0; kk < 2; ++kk) {
             const int m = 4 * kk + kq;
-            const double aF0 = (double)gU[v * PP + P * gq + T::f0pos(m, gq)];  // F0 at node (m, j = gq)
-            const double dg = sdg[gq + P * m];                               // dgM(m, gq)
-            const double bF1 = (double)gF1[v * PP + P * m + gq];             // F1 at node (i = gq, m)
+            const bool in = (P == 8) || (gq < P && m < P);  // the zero padding of P = 6
+            const double aF0 = in ? (double)bU[v * PP + P * gq + T::f0pos(m, gq)] : 0.0;  // F0 at (m, j = gq)
+            const double dg = in ? sdg[gq + P * m] : 0.0;                                  // dgM(m, gq)
+            const double bF = in ? (double)bF1[v * PP + P * m + gq] : 0.0;                // F1 at (i = gq, m)
             asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                          : "+d"(c0), "+d"(c1)
                          : "d"(aF0), "d"(dg));
             asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                          : "+d"(c0), "+d"(c1)
-                         : "d"(dg), "d"(bF1));
+                         : "d"(dg), "d"(bF));
           }
           dv[v][0] = c0;  // D(j = gq, i = 2 kq), D(gq, 2 kq + 1)
           dv[v][1] = c1;
         }
-        __syncwarp();  // the warp has read the xi flux it overwrites
+        if constexpr (EPG == 1) __syncwarp();  // the warp has read the xi flux it overwrites
         using R2 = typename std::conditional<sizeof(R) == 8, double2, float2>::type;
+        if (gq < P && 2 * kq + 1 < P) {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          R2 x;
-          x.x = (R)dv[v][0];
-          x.y = (R)dv[v][1];
-          reinterpret_cast<R2*>(gD + v * PP + P * gq)[kq] = x;
+          for (int v = 0; v < NV; ++v) {
+            R2 x;
+            x.x = (R)dv[v][0];
+            x.y = (R)dv[v][1];
+            reinterpret_cast<R2*>(bD + v * PP + P * gq)[kq] = x;
+          }
         }
       }
     } else {
