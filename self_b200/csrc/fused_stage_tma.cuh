@@ -100,8 +100,12 @@ struct TmaTraits {
   static_assert(TPE >= EPG * 4 * P, "the face phase gives each of the 4P face nodes its own thread");
   // 640 threads (five warps per scheduler at 96 registers) for P = 6 (ten
   // one-element or four four-element groups) and P = 8, up to 15 single-warp
-  // groups for P <= 4 (named barriers 1..15; barrier 0 is the CTA-wide one)
-  static constexpr int kMaxGroups = (P <= 4) ? 15 : (P == 6 ? 640 / TPE : 10);
+  // groups for P <= 4 (named barriers 1..15; barrier 0 is the CTA-wide one).
+  // ShallowWater FP64 at P = 6 runs three four-element groups at 128
+  // registers instead: at 96 it spills (measured 108.5 against 113.5 us per
+  // stage on 256x256; the other P = 6 forms are faster with four groups).
+  static constexpr int kMaxGroups =
+      (P <= 4) ? 15 : (P == 6 ? ((EPG == 4 && Phys::kLaggedVelocity && sizeof(R) == 8) ? 3 : 640 / TPE) : 10);
   static constexpr int kThreadsMax = kMaxGroups * TPE;
   // Per-element compute arrays (bulk type), laid out for conflict-free shared
   // accesses.  A 64-bit shared access is served per half-warp: two threads of
@@ -155,6 +159,13 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   constexpr int FS = T::FS, SS = T::SS, EPG = T::EPG, EB = T::EB;
   constexpr bool kLSW = (NV == 3 && !Phys::kLaggedVelocity);
   constexpr bool kSW = Phys::kLaggedVelocity;
+  // Neighbour traces loaded before phase A (measured per configuration: a
+  // gain at P = 8 and for ShallowWater FP64 at P = 6; a loss where the
+  // registers they hold across phase A make the kernel spill or crowd it --
+  // reference-rounding CompressibleIdealGas2D at P = 8, CompressibleIdealGas2D
+  // at P = 6, every model at P = 4)
+  constexpr bool kNbrEarly =
+      (P == 8) ? !(NV == 4 && ref_rounding<R>()) : (P == 6 && kSW && sizeof(R) == 8);
   extern __shared__ __align__(128) unsigned char smem[];
   const int C = pl.groups;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
@@ -328,6 +339,38 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       }
     };
 
+    // Face threads of this tile (phase C): each serves one face node of one
+    // element.  Their neighbour traces (and, ShallowWater, the neighbour's
+    // lagged velocity traces) are plain global loads; where kNbrEarly they
+    // are issued here, before phase A, so that their latency overlaps the
+    // flux computation, otherwise at the start of phase C.
+    const int c0 = TPE - EPG * 4 * P;  // first face thread of a multi-element group
+    const int cf = (EPG == 1) ? (t & 31) : t - c0;
+    const int eC = cf / (4 * P);
+    const bool faceOn = ((EPG == 1) ? ((t >> 5) == faceWarp && (t & 31) < 4 * P) : (t >= c0)) && eC < nLive;
+    const int cc = cf - eC * 4 * P;
+    const int s1 = cc / P, ii = cc % P;
+    const unsigned char* recC = sl + pl.oDsdx + (size_t)eC * gb;
+    const int* ssi = reinterpret_cast<const int*>(recC + rSi) + 5 * s1;
+    R X[NT], velR[2] = {(R)0, (R)0};
+    auto load_neighbour = [&]() {
+      const long long nb =
+          (ssi[4] == 0) ? (long long)TS * (ssi[3] / 10 - 1 + 4 * (long long)(ssi[2] - 1)) : -1;
+      const int i2 = (ssi[3] % 10) ? N - ii : ii;
+      const R* nbr = reinterpret_cast<const R*>(a.trIn) + (nb < 0 ? 0 : nb);
+#pragma unroll
+      for (int kf = 0; kf < NT; ++kf) X[kf] = (nb >= 0) ? nbr[i2 + P * kf] : (R)0;
+      if constexpr (kSW)
+        if (nb >= 0) {
+          const R* vn = reinterpret_cast<const R*>(a.velIn) +
+                        (size_t)2 * P * (ssi[3] / 10 - 1 + 4 * (size_t)(ssi[2] - 1));
+          velR[0] = vn[i2];
+          velR[1] = vn[i2 + P];
+        }
+    };
+    if constexpr (kNbrEarly)
+      if (faceOn) load_neighbour();
+
     // ---- A: flux auxiliaries, contravariant flux.  The buffer stays valid
     // until the end of phase D, so the solution, J and the node auxiliaries
     // are read again where they are needed instead of living in registers
@@ -375,8 +418,43 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     // 8x8 shape; FP32-bulk fluxes are widened exactly to FP64 and the sums
     // rounded back once).  The order of the additions inside a product is the
     // hardware's, so only the forms without the reference's rounding use it.
+    // At P = 4 one product covers both elements of a tile: rows and columns
+    // 0-3 belong to the first element, 4-7 to the second; the xi product's
+    // A rows and the eta product's B columns carry the element's flux, the
+    // dgMatrix operand is the same for both, and the two diagonal 4x4 blocks
+    // of the sum are the two elements' sums (the off-diagonal ones mix the
+    // elements and are dropped).
     constexpr bool kDmma = ((P == 8 && EPG == 1) || P == 6) && !ref_rounding<R>();
-    if constexpr (kDmma) {
+    constexpr bool kDmma4 = (P == 4 && EPG == 2 && TPE == 32) && !ref_rounding<R>();
+    if constexpr (kDmma4) {
+      const int lane = t & 31, gq = lane >> 2, kq = lane & 3;
+      const int eR = gq >> 2, jr = gq & 3;   // the element and node row of this lane's A row / B column
+      const R* bU = gBase + eR * EB;
+      const R* bF1 = bU + NV * PP;
+      const double dg = sdg[jr + P * kq];     // dgM(m = kq, jr): B of the xi product, A of the eta product
+      // this lane's sums: row gq, columns 2 kq, 2 kq + 1 -> element kq >> 1
+      const bool diag = (eR == (kq >> 1)) && eR < nLive;
+      R* bD = gBase + EPG * EB + eR * NV * PP;
+      using R2 = typename std::conditional<sizeof(R) == 8, double2, float2>::type;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        double c0 = 0.0, c1 = 0.0;
+        const double aF0 = (double)bU[v * PP + P * jr + T::f0pos(kq, jr)];  // F0 at (m = kq, j = jr)
+        const double bF = (double)bF1[v * PP + P * kq + jr];               // F1 at (i = jr, m = kq)
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                     : "+d"(c0), "+d"(c1)
+                     : "d"(aF0), "d"(dg));
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                     : "+d"(c0), "+d"(c1)
+                     : "d"(dg), "d"(bF));
+        if (diag) {  // D(j = jr, i = 2 (kq & 1)), D(jr, 2 (kq & 1) + 1)
+          R2 x;
+          x.x = (R)c0;
+          x.y = (R)c1;
+          reinterpret_cast<R2*>(bD + v * PP + P * jr)[kq & 1] = x;
+        }
+      }
+    } else if constexpr (kDmma) {
       // the warps a tile's face threads leave free take its elements in turn
       // (a one-element group: the warp that is not the face warp)
       constexpr int kDW = (EPG == 1) ? 1 : ((TPE - EPG * 4 * P) / 32 > 0 ? (TPE - EPG * 4 * P) / 32 : 1);
@@ -493,32 +571,18 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       }
     }
 
-    // ---- C: faces; own traces of this stage's solution come from the cache
+    // ---- C: faces; own traces of this stage's solution come from the cache,
+    // the neighbour's were loaded before phase A
     {
-      const int c0 = TPE - EPG * 4 * P;  // first face thread of a two-element group
-      const bool mine = (EPG == 1) ? ((t >> 5) == faceWarp && (t & 31) < 4 * P) : (t >= c0);
-      const int cf = (EPG == 1) ? (t & 31) : t - c0;
-      const int eC = cf / (4 * P);
-      if (mine && eC < nLive) {
-        const int cc = cf - eC * 4 * P;
-        const int s1 = cc / P, ii = cc % P;
+      if (faceOn) {
+        if constexpr (!kNbrEarly) load_neighbour();
         const long long eF = e0 + eC;
-        const unsigned char* recC = sl + pl.oDsdx + (size_t)eC * gb;
-        const int* ssi = reinterpret_cast<const int*>(recC + rSi);
-        const int bcid = ssi[5 * s1 + 4];
-        const bool physical = (bcid != 0) && (ssi[5 * s1 + 2] == 0);
-        const int flip = ssi[5 * s1 + 3] % 10;
+        const int bcid = ssi[4];
+        const bool physical = (bcid != 0) && (ssi[2] == 0);
         const R* own = reinterpret_cast<const R*>(sl + pl.oOwn + (size_t)eC * ob) + s1 * TS;
-        const int i2 = flip ? N - ii : ii;
-        const long long nb =
-            (bcid == 0) ? (long long)TS * (ssi[5 * s1 + 3] / 10 - 1 + 4 * (long long)(ssi[5 * s1 + 2] - 1)) : -1;
-        const R* nbr = reinterpret_cast<const R*>(a.trIn) + (nb < 0 ? 0 : nb);
-        R L[NT], X[NT];
+        R L[NT];
 #pragma unroll
-        for (int kf = 0; kf < NT; ++kf) {
-          L[kf] = own[ii + P * kf];
-          X[kf] = (nb >= 0) ? nbr[i2 + P * kf] : (R)0;
-        }
+        for (int kf = 0; kf < NT; ++kf) L[kf] = own[ii + P * kf];
         const double2 nh = reinterpret_cast<const double2*>(recC + rNhat)[ii + P * s1];
         const double ns = reinterpret_cast<const double*>(recC + rNs)[ii + P * s1];
         double fx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -541,25 +605,25 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
             fx[8] = pd[b + 2 * P];
           }
         }
-        R velL[2] = {(R)0, (R)0}, velR[2] = {(R)0, (R)0};
+        R velL[2] = {(R)0, (R)0};
         if constexpr (kSW) {
           const R* vo = reinterpret_cast<const R*>(sl + pl.oVelOwn + (size_t)eC * vb);
           velL[0] = vo[ii + P * (0 + 2 * s1)];
           velL[1] = vo[ii + P * (1 + 2 * s1)];
-          if (nb >= 0) {  // the neighbour's stage-lagged velocity traces, plain loads
-            const R* vn = reinterpret_cast<const R*>(a.velIn) +
-                          (size_t)2 * P * (ssi[5 * s1 + 3] / 10 - 1 + 4 * (size_t)(ssi[5 * s1 + 2] - 1));
-            velR[0] = vn[i2];
-            velR[1] = vn[i2 + P];
-          }
           R* vOut = reinterpret_cast<R*>(a.velOut);
-          vOut[ii + P * (0 + 2 * (s1 + 4 * eF))] = L[0] / L[2];
-          vOut[ii + P * (1 + 2 * (s1 + 4 * eF))] = L[1] / L[2];
+          if constexpr (ref_rounding<R>()) {
+            vOut[ii + P * (0 + 2 * (s1 + 4 * eF))] = L[0] / L[2];
+            vOut[ii + P * (1 + 2 * (s1 + 4 * eF))] = L[1] / L[2];
+          } else {
+            const R rH = (R)1 / L[2];
+            vOut[ii + P * (0 + 2 * (s1 + 4 * eF))] = L[0] * rH;
+            vOut[ii + P * (1 + 2 * (s1 + 4 * eF))] = L[1] * rH;
+          }
         }
         R out[NV];
         Phys::template face<R>(bcid, physical, L, X, velL, velR, nh.x, nh.y, ns, fx, a, out);
         if constexpr (NV == 4)
-          if (a.av) av_face_add<P, R>(a, s1, ii, eF, ssi + 5 * s1, nh.x, nh.y, ns, out);
+          if (a.av) av_face_add<P, R>(a, s1, ii, eF, ssi, nh.x, nh.y, ns, out);
         R* fb = gBase + eC * EB + T::kU;
 #pragma unroll
         for (int v = 0; v < NV; ++v) fb[s1 * SS + v * P + ii] = out[v];
@@ -643,7 +707,10 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     // so that for P = 8 a half-warp reads the column lines (or the row lines)
     // of two fields.
     {
-      constexpr int NTp = (NT + 1) / 2 * 2;
+      // P = 8 numbers the tasks by field pair (an odd NT leaves the last
+      // pair's second half idle); the padded layouts of the other P number
+      // them by orientation, field, line, with no idle tasks
+      constexpr int NTp = T::kSwz ? (NT + 1) / 2 * 2 : NT;
       constexpr int TPEl = 2 * NTp * P;  // tasks per element
       // a one-element group's face warp starts one warp later, so the other
       // warp takes the last, partial round
@@ -651,9 +718,19 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       for (int kk = k0; kk < EPG * TPEl; kk += TPE) {
         const int eE = kk / TPEl, ks = kk - eE * TPEl;
         if (eE >= nLive) continue;
-        const int fp = ks / (4 * P), r = ks - fp * 4 * P, row = r / (2 * P), r2 = r - row * 2 * P, fs = r2 / P;
-        const int l = r2 - fs * P, fi = 2 * fp + fs;
-        if (fi >= NT) continue;
+        int row, fi, l;
+        if constexpr (T::kSwz) {
+          const int fp = ks / (4 * P), r = ks - fp * 4 * P, r2 = r - (r / (2 * P)) * 2 * P, fs = r2 / P;
+          row = r / (2 * P);
+          l = r2 - fs * P;
+          fi = 2 * fp + fs;
+          if (fi >= NT) continue;
+        } else {
+          row = ks / (NT * P);
+          const int r = ks - row * NT * P;
+          fi = r / P;
+          l = r - fi * P;
+        }
         const R* fv = gBase + eE * EB + fi * FS;
         R lo = (R)0, hi = (R)0;
 #pragma unroll
