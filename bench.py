@@ -327,15 +327,20 @@ def run_forms(steps=500, err_steps=500, n_instances=256):
     inst = E.make_instances(n_instances, seed=0)
     e64 = E.ShallowWaterEnsemble(inst, form=S.FP64, autotune=True)
     e32 = E.ShallowWaterEnsemble(inst, form=S.FP32_BULK, autotune=True)
+    # the same FP64 kernels, each degree's handle replaying its own graph on its stream
+    e64s = E.ShallowWaterEnsemble(inst, form=S.FP64, autotune=False, one_graph=False)
+    for N, tun in e64.tuning.items():
+        S.lib().selfgpu_model2d_set_launch(e64s.handles[N]["model"]._h, tun["persistent"], tun["groups"])
     un = E.UnbatchedShallowWater(inst)
     dof = sum(i.dof() for i in inst)
     out = {"workload": f"{n_instances} ShallowWater instances, nx,ny~U{{8..64}}, N~U{{3,5,7}}, FP32/FP64, "
-                       f"per-instance CFL 0.5; rates over {steps} RK3 steps", "dof": dof}
-    for name, runner in (("unbatched_fp64", un), ("batched_fp64", e64), ("batched_fp32_bulk", e32)):
+                       f"per-instance CFL 0.5; rates over {steps} RK3 steps", "dof": dof,
+           "batched_launch": "one CUDA graph launch per RK3 step for all degrees (one branch per degree)"}
+    for name, runner in (("unbatched_fp64", un), ("batched_fp64", e64), ("batched_fp32_bulk", e32),
+                         ("batched_fp64_per_degree_streams", e64s)):
         runner.reset()
         runner.ForwardStep(2)
         torch.cuda.synchronize()
-        l0 = runner.launches() if hasattr(runner, "launches") else None
         t = E.time_it(lambda: runner.ForwardStep(steps))
         out[name] = {"value": dof * steps / t, "unit": "DOF-updates/s", "ms_per_rk3_step": 1e3 * t / steps}
     out["speedup_fp32_batched_vs_unbatched_fp64"] = out["batched_fp32_bulk"]["value"] / out["unbatched_fp64"]["value"]

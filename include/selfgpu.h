@@ -343,6 +343,19 @@ int selfgpu_model2d_set_multistep(selfgpu_model2d* m, int enable);
  * and the persistent kernel's consumer-group cap (0 = as many as fit). */
 int selfgpu_model2d_set_launch(selfgpu_model2d* m, int persistent, int groups);
 
+/* Ensembles: n handles (each ready to step; typically one per degree of an
+ * uneven batch, every element carrying its instance's dt) advanced together.
+ * selfgpu_ensemble_rk3 runs nSteps RK3 steps of every handle as ONE CUDA
+ * graph launch per step on the ensemble's stream (NULL at create: its own);
+ * the graph has one branch per handle, so the handles' stage kernels run
+ * concurrently.  Results equal selfgpu_model2d_rk3 on each handle bit for
+ * bit.  Work issued earlier on the handles' streams runs first, and later
+ * work on them waits for the steps.  The handles must outlive the ensemble. */
+typedef struct selfgpu_ensemble selfgpu_ensemble;
+int selfgpu_ensemble_create(selfgpu_model2d* const* handles, int n, void* stream, selfgpu_ensemble** out);
+int selfgpu_ensemble_rk3(selfgpu_ensemble* e, double dt, int nSteps);
+int selfgpu_ensemble_destroy(selfgpu_ensemble* e);
+
 /* Autotuner: times the per-element-group kernel and the persistent kernel at
  * every consumer-group count that fits (elements in flight per CTA, each with
  * its double-buffered staging tile) on RK-stage launches over this handle's

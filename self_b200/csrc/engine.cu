@@ -253,7 +253,10 @@ struct selfgpu_model2d {
     return cudaSuccess;
   }
 
+  unsigned long long gen = 0;  // bumped whenever captured work goes stale (ensemble graphs check it)
+
   void drop_graphs() {
+    ++gen;
     for (auto& row : graph)
       for (auto& g : row)
         if (g) {
@@ -1039,5 +1042,189 @@ int selfgpu_integral_mapped_scalar2d(const double* interior, int iVar, int nVar,
 }
 
 long long selfgpu_model2d_launch_count(const selfgpu_model2d* m) { return m ? m->launches : 0; }
+
+}  // extern "C"
+
+// ----------------------------------------------------------------- ensembles
+// Several handles advanced together: one RK step of all of them is ONE CUDA
+// graph whose branches (one per handle, each on its own capture stream) hold
+// that handle's stage launches, so the handles' kernels run concurrently and
+// the whole ensemble costs one graph launch per step.  Captured per joint
+// buffer parity of the handles (the parities flip every step, so two graphs
+// serve a run) and re-captured when dt or any handle's launch state changes.
+struct selfgpu_ensemble {
+  std::vector<selfgpu_model2d*> h;
+  cudaStream_t stream = nullptr;  // the stream the graph is launched on
+  bool ownStream = false;
+  std::vector<cudaStream_t> branch;  // capture streams, one per handle
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  struct Entry {
+    std::vector<int> key;                  // (cur, vcur) of every handle at the step's start
+    std::vector<unsigned long long> gen;   // handle generations at capture
+    std::vector<long long> launches, tma;  // per handle and step
+    double dt = NAN;
+    cudaGraphExec_t g = nullptr;
+  };
+  std::vector<Entry> cache;
+
+  std::vector<int> key() const {
+    std::vector<int> k(h.size());
+    for (size_t i = 0; i < h.size(); ++i) k[i] = h[i]->cur | (h[i]->vcur << 1);
+    return k;
+  }
+  void drop() {
+    for (auto& c : cache)
+      if (c.g) cudaGraphExecDestroy(c.g);
+    cache.clear();
+  }
+  Entry* find(double dt) {
+    const std::vector<int> k = key();
+    for (auto& c : cache) {
+      if (c.key != k || !(c.dt == dt)) continue;
+      bool fresh = true;
+      for (size_t i = 0; i < h.size(); ++i) fresh = fresh && c.gen[i] == h[i]->gen;
+      if (fresh) return &c;
+    }
+    return nullptr;
+  }
+  // capture one step of every handle from the current parities (restored afterwards)
+  cudaError_t capture(double dt, Entry& out) {
+    const size_t n = h.size();
+    out.key = key();
+    out.gen.resize(n);
+    out.launches.assign(n, 0);
+    out.tma.assign(n, 0);
+    out.dt = dt;
+    std::vector<int> c0(n), v0(n);
+    std::vector<cudaStream_t> s0(n);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    e = cudaEventRecord(fork, stream);
+    for (size_t i = 0; i < n && e == cudaSuccess; ++i) {
+      selfgpu_model2d* m = h[i];
+      c0[i] = m->cur;
+      v0[i] = m->vcur;
+      s0[i] = m->stream;
+      out.gen[i] = m->gen;
+      e = cudaStreamWaitEvent(branch[i], fork, 0);
+      if (e != cudaSuccess) break;
+      m->stream = branch[i];
+      const long long l0 = m->launches, t0 = m->tmaLaunches;
+      e = m->step(dt);
+      out.launches[i] = m->launches - l0;
+      out.tma[i] = m->tmaLaunches - t0;
+      m->launches = l0;
+      m->tmaLaunches = t0;
+      m->stream = s0[i];
+      m->cur = c0[i];
+      m->vcur = v0[i];
+      if (e == cudaSuccess) e = cudaEventRecord(join[i], branch[i]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, join[i], 0);
+    }
+    cudaError_t e2 = cudaStreamEndCapture(stream, &graph);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&out.g, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      out.g = nullptr;
+    }
+    return e;
+  }
+};
+
+extern "C" {
+
+int selfgpu_ensemble_create(selfgpu_model2d* const* handles, int n, void* stream, selfgpu_ensemble** out) {
+  if (!handles || n < 1 || !out) return set_error(SELFGPU_ERR_ARG, "selfgpu_ensemble_create: bad arguments");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (!handles[i]) return set_error(SELFGPU_ERR_ARG, "selfgpu_ensemble_create: null handle");
+    for (int k = 0; k < i; ++k)
+      if (handles[k] == handles[i]) return set_error(SELFGPU_ERR_ARG, "selfgpu_ensemble_create: repeated handle");
+  }
+  auto* x = new selfgpu_ensemble();
+  x->h.assign(handles, handles + n);
+  cudaError_t e = cudaSuccess;
+  if (stream) {
+    x->stream = (cudaStream_t)stream;
+  } else {
+    e = cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking);
+    x->ownStream = e == cudaSuccess;
+  }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&x->fork, cudaEventDisableTiming);
+  x->branch.assign(n, nullptr);
+  x->join.assign(n, nullptr);
+  for (int i = 0; i < n && e == cudaSuccess; ++i) {
+    e = cudaStreamCreateWithFlags(&x->branch[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&x->join[i], cudaEventDisableTiming);
+  }
+  if (e != cudaSuccess) {
+    selfgpu_ensemble_destroy(x);
+    return fail_cuda("selfgpu_ensemble_create", e);
+  }
+  *out = x;
+  return SELFGPU_OK;
+}
+
+int selfgpu_ensemble_destroy(selfgpu_ensemble* x) {
+  if (!x) return SELFGPU_OK;
+  if (x->stream) cudaStreamSynchronize(x->stream);
+  x->drop();
+  for (auto s : x->branch)
+    if (s) cudaStreamDestroy(s);
+  for (auto ev : x->join)
+    if (ev) cudaEventDestroy(ev);
+  if (x->fork) cudaEventDestroy(x->fork);
+  if (x->ownStream) cudaStreamDestroy(x->stream);
+  delete x;
+  return SELFGPU_OK;
+}
+
+int selfgpu_ensemble_rk3(selfgpu_ensemble* x, double dt, int nSteps) {
+  if (!x || nSteps < 0) return set_error(SELFGPU_ERR_ARG, "selfgpu_ensemble_rk3: bad arguments");
+  const size_t n = x->h.size();
+  for (auto m : x->h) {
+    int rc = check_ready(m, "selfgpu_ensemble_rk3");
+    if (rc) return rc;
+  }
+  if (nSteps == 0) return SELFGPU_OK;
+  cudaError_t e = cudaSuccess;
+  // work already issued on the handles' streams (prologues included) comes first
+  for (size_t i = 0; i < n && e == cudaSuccess; ++i) {
+    selfgpu_model2d* m = x->h[i];
+    if (!m->valid) e = m->prologue();
+    if (e == cudaSuccess) e = cudaEventRecord(x->join[i], m->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(x->stream, x->join[i], 0);
+  }
+  if (e != cudaSuccess) return fail_cuda("selfgpu_ensemble_rk3", e);
+  for (int s = 0; s < nSteps; ++s) {
+    selfgpu_ensemble::Entry* c = x->find(dt);
+    if (!c) {
+      if (x->cache.size() >= 4) x->drop();
+      selfgpu_ensemble::Entry fresh;
+      e = x->capture(dt, fresh);
+      if (e != cudaSuccess) return fail_cuda("selfgpu_ensemble_rk3: capture", e);
+      x->cache.push_back(std::move(fresh));
+      c = &x->cache.back();
+    }
+    e = cudaGraphLaunch(c->g, x->stream);
+    if (e != cudaSuccess) return fail_cuda("selfgpu_ensemble_rk3: graph launch", e);
+    for (size_t i = 0; i < n; ++i) {
+      selfgpu_model2d* m = x->h[i];
+      m->launches += c->launches[i];
+      m->tmaLaunches += c->tma[i];
+      m->cur = 1 - m->cur;  // three swaps per step
+      if (m->model == SELFGPU_MODEL_SW) m->vcur = 1 - m->vcur;
+    }
+  }
+  // later work on the handles' streams waits for the steps
+  e = cudaEventRecord(x->fork, x->stream);
+  for (size_t i = 0; i < n && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(x->h[i]->stream, x->fork, 0);
+  if (e != cudaSuccess) return fail_cuda("selfgpu_ensemble_rk3", e);
+  return SELFGPU_OK;
+}
 
 }  // extern "C"

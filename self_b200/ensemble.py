@@ -101,9 +101,13 @@ def arc_lengths(geo, N):
 
 class _Ensemble:
     """Instances grouped by degree; one fused handle per degree on its own
-    stream.  Subclasses build a group's model (_build_group)."""
+    stream.  ForwardStep advances every handle with one CUDA graph launch per
+    RK step (selfgpu_ensemble_rk3: one graph branch per degree, so the
+    degrees' kernels run concurrently), or, with one_graph=False, each handle
+    replays its own captured step on its stream.  Subclasses build a group's
+    model (_build_group)."""
 
-    def __init__(self, instances, form, autotune, shared_stream=False):
+    def __init__(self, instances, form, autotune, shared_stream=False, one_graph=True):
         self.instances, self.form = instances, form
         self.groups = {}
         for inst in instances:
@@ -120,6 +124,8 @@ class _Ensemble:
             h["q0"] = h["model"].solution.clone()
             torch.cuda.synchronize()
             self.handles[N] = h
+        self.one_graph = one_graph
+        self._ens = None
         self.tuning = {}
         if autotune:
             for N, h in self.handles.items():
@@ -135,9 +141,29 @@ class _Ensemble:
                 h["model"].workSol.zero_()
         torch.cuda.synchronize()
 
+    def _ensemble(self):
+        if self._ens is None:
+            hs = [h["model"]._h for h in self.handles.values()]
+            arr = (A.ctypes.c_void_p * len(hs))(*hs)
+            out = A.ctypes.c_void_p()
+            check(lib().selfgpu_ensemble_create(arr, len(hs), None, A.ctypes.byref(out)))
+            self._ens = out
+        return self._ens
+
+    def close(self):
+        if getattr(self, "_ens", None) is not None:
+            lib().selfgpu_ensemble_destroy(self._ens)
+            self._ens = None
+
+    def __del__(self):
+        self.close()
+
     def ForwardStep(self, nSteps):
-        """nSteps RK3 steps of every instance (each with its own dt); the
-        per-degree handles run concurrently on their streams."""
+        """nSteps RK3 steps of every instance (each with its own dt), the
+        per-degree handles' kernels running concurrently."""
+        if self.one_graph:
+            check(lib().selfgpu_ensemble_rk3(self._ensemble(), 0.0, int(nSteps)))
+            return
         for h in self.handles.values():
             with torch.cuda.stream(h["stream"]):
                 check(lib().selfgpu_model2d_rk3(h["model"]._h, 0.0, int(nSteps)))
@@ -156,9 +182,10 @@ class _Ensemble:
 class ShallowWaterEnsemble(_Ensemble):
     """Batched ShallowWater instances."""
 
-    def __init__(self, instances, form=A.FP32_BULK, cfl=0.5, autotune=True, g=1.0, shared_stream=False):
+    def __init__(self, instances, form=A.FP32_BULK, cfl=0.5, autotune=True, g=1.0, shared_stream=False,
+                 one_graph=True):
         self.cfl, self.g = cfl, g
-        super().__init__(instances, form, autotune, shared_stream)
+        super().__init__(instances, form, autotune, shared_stream, one_graph)
 
     @staticmethod
     def _instance_mesh(inst):
@@ -315,9 +342,10 @@ class CompressibleGasEnsemble(_Ensemble):
     (closure = CLOSURE_OFF / CLOSURE_INDICATOR / CLOSURE_MLP; mlps maps a
     degree to its ClosureMLP)."""
 
-    def __init__(self, instances, form=A.FP32_BULK, closure=A.CLOSURE_OFF, mlps=None, c_av=1.0, autotune=True):
+    def __init__(self, instances, form=A.FP32_BULK, closure=A.CLOSURE_OFF, mlps=None, c_av=1.0, autotune=True,
+                 one_graph=True):
         self.closure, self.mlps, self.c_av = closure, mlps or {}, c_av
-        super().__init__(instances, form, autotune)
+        super().__init__(instances, form, autotune, one_graph=one_graph)
 
     @staticmethod
     def _instance_mesh(inst):

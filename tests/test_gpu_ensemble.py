@@ -149,3 +149,72 @@ def test_gas_ensemble_fp32_learned_error_on_smooth_members(capsys):
         print(f"\nFP32-bulk + learned-closure gas ensemble: worst relative L2 error vs FP64 on smooth members "
               f"after {n} steps = {worst:.3e}")
     assert 0.0 < worst < 1e-6
+
+
+@pytest.mark.parametrize("form_name", ["FP64", "FP64_REF", "FP32_BULK"])
+def test_one_graph_equals_per_handle_replay(form_name):
+    """One graph launch per RK step for the whole ensemble (one branch per
+    degree) gives the per-handle graph replays' results bit for bit, across
+    calls of different lengths, a reset and re-autotuned handles."""
+    import self_b200 as S
+    from self_b200 import ensemble as E
+    form = getattr(S, form_name)
+    inst = _small_instances(seed=8)
+    one = E.ShallowWaterEnsemble(inst, form=form, autotune=True, one_graph=True)
+    per = E.ShallowWaterEnsemble(inst, form=form, autotune=False, one_graph=False)
+    for N, h in one.handles.items():  # the same kernel variants in both
+        t = one.tuning[N]
+        S.lib().selfgpu_model2d_set_launch(per.handles[N]["model"]._h, t["persistent"], t["groups"])
+    for n in (1, 4, 3):
+        one.ForwardStep(n)
+        per.ForwardStep(n)
+    torch.cuda.synchronize()
+    for it in inst:
+        a = one.solution(it).cpu().numpy()
+        assert np.isfinite(a).all()
+        np.testing.assert_array_equal(a, per.solution(it).cpu().numpy())
+    launches = one.launches()
+    assert launches == per.launches() and launches > 0
+    one.reset()
+    per.reset()
+    one.ForwardStep(5)
+    per.ForwardStep(5)
+    torch.cuda.synchronize()
+    for it in inst:
+        np.testing.assert_array_equal(one.solution(it).cpu().numpy(), per.solution(it).cpu().numpy())
+    one.close()
+
+
+def test_one_graph_gas_closure_equals_per_handle_replay():
+    """The closure kernels of every degree are captured into the same
+    ensemble graph (indicator closure, production FP64)."""
+    import self_b200 as S
+    from self_b200 import ensemble as E
+    inst = _gas_instances(seed=9)
+    one = E.CompressibleGasEnsemble(inst, form=S.FP64, closure=S.CLOSURE_INDICATOR, autotune=False,
+                                    one_graph=True)
+    per = E.CompressibleGasEnsemble(inst, form=S.FP64, closure=S.CLOSURE_INDICATOR, autotune=False,
+                                    one_graph=False)
+    one.ForwardStep(7)
+    per.ForwardStep(7)
+    torch.cuda.synchronize()
+    for it in inst:
+        a = one.solution(it).cpu().numpy()
+        assert np.isfinite(a).all()
+        np.testing.assert_array_equal(a, per.solution(it).cpu().numpy())
+
+
+def test_ensemble_create_rejects_bad_arguments():
+    import ctypes
+
+    import self_b200 as S
+    from self_b200._lib import lib
+    from self_b200 import ensemble as E
+    ens = E.ShallowWaterEnsemble(_small_instances(seed=10), form=S.FP64, autotune=False)
+    h = next(iter(ens.handles.values()))["model"]._h
+    out = ctypes.c_void_p()
+    arr = (ctypes.c_void_p * 2)(h, h)
+    assert lib().selfgpu_ensemble_create(arr, 2, None, ctypes.byref(out)) != 0  # repeated handle
+    assert lib().selfgpu_ensemble_create(arr, 0, None, ctypes.byref(out)) != 0
+    assert lib().selfgpu_ensemble_rk3(None, 0.0, 1) != 0
+    assert lib().selfgpu_ensemble_destroy(None) == 0
