@@ -10,9 +10,10 @@
 // With the closure on, each RK stage runs, before the stage kernel:
 //   k_av_nu     the element viscosity nu (modal-decay indicator of the
 //               density, or the closure MLP with the indicator as fallback and
-//               screen), and the list of elements with nu > 0: in FP32 one lane
-//               per element for the indicator, warp-wide for the few elements
-//               that need the MLP or the wave speed; in FP64 one warp per element;
+//               screen), and the list of elements with nu > 0: in FP32 (and
+//               FP64 up to P = 6) one lane per element for the indicator,
+//               warp-wide for the few elements that need the MLP or the wave
+//               speed; in FP64 at P > 6 one warp per element;
 //   k_av_grad   the listed elements only: the BR1 gradient of the four
 //               conservative variables from the averaged traces of the stage's
 //               trace cache, the contravariant viscous volume flux
@@ -341,10 +342,11 @@ __global__ void __launch_bounds__(32 * kNuWarps) k_av_nu(const AvArgs a) {
   __syncthreads();
   const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
   NuWarpSmem<P, R>& s = ws[w];
-  if constexpr (sizeof(R) == 4) {
-    // FP32: one lane per element for the indicator (the warp's 32 elements
-    // are spread over the mesh, so that the few that need the MLP or the wave
-    // speed, done warp-wide, are spread over the warps too)
+  if constexpr (sizeof(R) == 4 || P <= 6) {
+    // FP32, and FP64 up to P = 6 (its P^2 densities fit the registers): one
+    // lane per element for the indicator (the warp's 32 elements are spread
+    // over the mesh, so that the few that need the MLP or the wave speed,
+    // done warp-wide, are spread over the warps too)
     const long long nW = (long long)gridDim.x * kNuWarps;
     for (long long base = (long long)blockIdx.x * kNuWarps + w; base < a.nEl; base += 32 * nW) {
       const long long e = base + (long long)lane * nW;
@@ -430,7 +432,7 @@ __global__ void __launch_bounds__(32 * kNuWarps) k_av_nu(const AvArgs a) {
     }
     return;
   }
-  // FP64: one warp per element
+  // FP64 at P > 6: one warp per element
   // the density of the warp's next element is loaded into registers while
   // the current one is processed (the loads' latency is the main cost)
   constexpr int QPL = (PP + 31) / 32;  // density values per lane
