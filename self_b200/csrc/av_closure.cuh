@@ -10,10 +10,9 @@
 // With the closure on, each RK stage runs, before the stage kernel:
 //   k_av_nu     the element viscosity nu (modal-decay indicator of the
 //               density, or the closure MLP with the indicator as fallback and
-//               screen), and the list of elements with nu > 0: in FP32 (and
-//               FP64 up to P = 6) one lane per element for the indicator,
-//               warp-wide for the few elements that need the MLP or the wave
-//               speed; in FP64 at P > 6 one warp per element;
+//               screen), and the list of elements with nu > 0: one lane per
+//               element for the indicator, warp-wide for the few elements
+//               that need the MLP or the wave speed;
 //   k_av_grad   the listed elements only: the BR1 gradient of the four
 //               conservative variables from the averaged traces of the stage's
 //               trace cache, the contravariant viscous volume flux
@@ -151,10 +150,11 @@ __device__ void modal_features(const R* c, float* f) {
 }
 
 // ------------------------------------------------------ viscosity kernel
-// One warp per element (warp-level synchronisation only): density modes,
-// activation and screening; the MLP only where the indicator does not screen
-// the element out; the wave speed, the viscosity and an entry in the list of
-// active elements only where the activation is not zero.
+// One lane per element: density modes, activation and screening; then, warp
+// wide (warp-level synchronisation only) and only for the warp's elements
+// that need them, the MLP where the indicator does not screen the element
+// out, and the wave speed where the activation is not zero; the viscosity and
+// an entry in the list of active elements.
 template <int P, typename R>
 struct NuWarpSmem {
   static constexpr int PP = P * P;
@@ -162,7 +162,7 @@ struct NuWarpSmem {
   R tt[PP];
   R c[2][PP];  // modal energies c^2
   R part[3][P];
-  R act[32], lam[32];  // per lane's element (FP32 lane-per-element path)
+  R act[32], lam[32];  // per lane's element
   float feat[kMlpIn];
   float h1[kMlpHidden];
 };
@@ -342,11 +342,12 @@ __global__ void __launch_bounds__(32 * kNuWarps) k_av_nu(const AvArgs a) {
   __syncthreads();
   const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
   NuWarpSmem<P, R>& s = ws[w];
-  if constexpr (sizeof(R) == 4 || P <= 6) {
-    // FP32, and FP64 up to P = 6 (its P^2 densities fit the registers): one
-    // lane per element for the indicator (the warp's 32 elements are spread
-    // over the mesh, so that the few that need the MLP or the wave speed,
-    // done warp-wide, are spread over the warps too)
+  {
+    // One lane per element for the indicator (the warp's 32 elements are
+    // spread over the mesh, so that the few that need the MLP or the wave
+    // speed, done warp-wide, are spread over the warps too).  FP64 at P = 8
+    // holds 64 densities per lane and spills a little; still measured 7 %
+    // faster per C5 step than one warp per element.
     const long long nW = (long long)gridDim.x * kNuWarps;
     for (long long base = (long long)blockIdx.x * kNuWarps + w; base < a.nEl; base += 32 * nW) {
       const long long e = base + (long long)lane * nW;
@@ -430,63 +431,6 @@ __global__ void __launch_bounds__(32 * kNuWarps) k_av_nu(const AvArgs a) {
       }
       __syncwarp();
     }
-    return;
-  }
-  // FP64 at P > 6: one warp per element
-  // the density of the warp's next element is loaded into registers while
-  // the current one is processed (the loads' latency is the main cost)
-  constexpr int QPL = (PP + 31) / 32;  // density values per lane
-  const long long eStride = (long long)gridDim.x * kNuWarps;
-  double qn[QPL];
-  auto load_density = [&](long long e) {
-#pragma unroll
-    for (int r = 0; r < QPL; ++r) {
-      const int k = lane + 32 * r;
-      qn[r] = (e < a.nEl && k < PP) ? a.q[k + (long long)PP * (2 + 4 * e)] : 0.0;
-    }
-  };
-  load_density((long long)blockIdx.x * kNuWarps + w);
-  for (long long e = (long long)blockIdx.x * kNuWarps + w; e < a.nEl; e += eStride) {
-#pragma unroll
-    for (int r = 0; r < QPL; ++r)
-      if (lane + 32 * r < PP) s.q[0][lane + 32 * r] = (R)qn[r];
-    load_density(e + eStride);
-    __syncwarp();
-    warp_modal_energy<P, R>(sT, s.q[0], s.tt, s.c[0], lane);
-    // fixed-order sums per eta-degree l, then over l
-    if (lane < P) {
-      const int l = lane;
-      R tot = (R)0;
-#pragma unroll
-      for (int k = 0; k < P; ++k) tot = tot + s.c[0][k + P * l];
-      s.part[0][l] = tot;
-      s.part[1][l] = (l == N) ? tot : s.c[0][N + P * l];
-    }
-    __syncwarp();
-    R actInd = (R)0;
-    int need = 0;
-    if (lane == 0) {
-      R total = (R)0, top = (R)0;
-#pragma unroll
-      for (int l = 0; l < P; ++l) {
-        total = total + s.part[0][l];
-        top = top + s.part[1][l];
-      }
-      indicator_act<R>(a, total, top, mlp, actInd, need);
-    }
-    actInd = __shfl_sync(0xffffffffu, actInd, 0);
-    need = __shfl_sync(0xffffffffu, need, 0);
-    __syncwarp();
-    const R act = need ? warp_mlp_act<P, R>(a, sT, s, sW1, sW2, sw3, sB, e, lane, actInd) : actInd;
-    double nu = 0.0;
-    if (act != (R)0) nu = (double)act * a.avC * a.hEl[e] / (double)N * (double)warp_wave_speed<P, R>(a, e, lane);
-    if (lane == 0) {
-      a.nu[e] = nu;
-      a.act[e] = (float)act;
-      if (mlp && a.actInd) a.actInd[e] = (float)actInd;
-      if (nu != 0.0) a.activeList[atomicAdd(a.activeCount, 1)] = (int)e;
-    }
-    __syncwarp();
   }
 }
 
