@@ -166,6 +166,20 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   // at P = 6, every model at P = 4)
   constexpr bool kNbrEarly =
       (P == 8) ? !(NV == 4 && ref_rounding<R>()) : (P == 6 && kSW && sizeof(R) == 8);
+  // divergence sums as FP64 tensor-core products (phase B): production and
+  // FP32-bulk forms at P = 8 and 6 (one element per warp) and 4 (two)
+  constexpr bool kDmma = ((P == 8 && EPG == 1) || P == 6) && !ref_rounding<R>();
+  constexpr bool kDmma4 = (P == 4 && EPG == 2 && TPE == 32) && !ref_rounding<R>();
+  // At P = 8 the products' operand loads read, per half-warp, four rows of
+  // the xi flux, the eta flux and the transposed dgMatrix at four columns
+  // each; rows two apart would share banks, so these three arrays keep the
+  // column index XOR 4 in row pairs 2-3 and 6-7 (the per-node stores of
+  // phase A stay conflict-free, as a half-warp stores two whole rows).
+  constexpr bool kSw8 = (P == 8) && kDmma;
+  auto cswz = [](int c, int r) { return kSw8 ? (c ^ (4 * ((r >> 1) & 1))) : c; };
+  auto f0at = [&](int m, int j) { return kSw8 ? P * j + cswz(m, j) : P * j + T::f0pos(m, j); };  // F0(m, j)
+  auto f1at = [&](int i, int j) { return P * j + cswz(i, j); };                                  // F1(i, j)
+  auto dgat = [&](int m, int i) { return P * m + cswz(i, m); };                                  // dgM(m, i)
   extern __shared__ __align__(128) unsigned char smem[];
   const int C = pl.groups;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
@@ -180,9 +194,10 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     for (int k = 0; k < 2 * C; ++k) mbar_init(&full[k], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  // dgMatrix transposed (sdg[i + P m] = dgM(m, i)): a warp's reads of the
-  // columns of its nodes' i (or j) are then consecutive
-  for (int k = threadIdx.x; k < PP; k += blockDim.x) sdg[k] = a.dgM[k / P + P * (k % P)];
+  // dgMatrix transposed (sdg[i + P m] = dgM(m, i), the column index swizzled
+  // where kSw8): a warp's reads of the columns of its nodes' i (or j) are then
+  // consecutive
+  for (int k = threadIdx.x; k < PP; k += blockDim.x) sdg[dgat(k / P, k % P)] = a.dgM[k / P + P * (k % P)];
   for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) sb[k] = a.bM[k];
   for (int k = threadIdx.x; k < P; k += blockDim.x) {
     sqw[k] = a.qw[k];
@@ -397,8 +412,8 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         if (a.av) av_volume_add<P, R>(a, n, e, F0, F1);
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        gU[v * PP + P * j + T::f0pos(i, j)] = F0[v];
-        gF1[v * PP + n] = F1[v];
+        gU[v * PP + f0at(i, j)] = F0[v];
+        gF1[v * PP + f1at(i, j)] = F1[v];
       }
     }
     named_bar(barId, TPE);  // contravariant fluxes ready
@@ -424,14 +439,12 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     // dgMatrix operand is the same for both, and the two diagonal 4x4 blocks
     // of the sum are the two elements' sums (the off-diagonal ones mix the
     // elements and are dropped).
-    constexpr bool kDmma = ((P == 8 && EPG == 1) || P == 6) && !ref_rounding<R>();
-    constexpr bool kDmma4 = (P == 4 && EPG == 2 && TPE == 32) && !ref_rounding<R>();
     if constexpr (kDmma4) {
       const int lane = t & 31, gq = lane >> 2, kq = lane & 3;
       const int eR = gq >> 2, jr = gq & 3;   // the element and node row of this lane's A row / B column
       const R* bU = gBase + eR * EB;
       const R* bF1 = bU + NV * PP;
-      const double dg = sdg[jr + P * kq];     // dgM(m = kq, jr): B of the xi product, A of the eta product
+      const double dg = sdg[dgat(kq, jr)];    // dgM(m = kq, jr): B of the xi product, A of the eta product
       // this lane's sums: row gq, columns 2 kq, 2 kq + 1 -> element kq >> 1
       const bool diag = (eR == (kq >> 1)) && eR < nLive;
       R* bD = gBase + EPG * EB + eR * NV * PP;
@@ -439,8 +452,8 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
         double c0 = 0.0, c1 = 0.0;
-        const double aF0 = (double)bU[v * PP + P * jr + T::f0pos(kq, jr)];  // F0 at (m = kq, j = jr)
-        const double bF = (double)bF1[v * PP + P * kq + jr];               // F1 at (i = jr, m = kq)
+        const double aF0 = (double)bU[v * PP + f0at(kq, jr)];  // F0 at (m = kq, j = jr)
+        const double bF = (double)bF1[v * PP + f1at(jr, kq)];   // F1 at (i = jr, m = kq)
         asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                      : "+d"(c0), "+d"(c1)
                      : "d"(aF0), "d"(dg));
@@ -473,9 +486,9 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
           for (int kk = 0; kk < 2; ++kk) {
             const int m = 4 * kk + kq;
             const bool in = (P == 8) || (gq < P && m < P);  // the zero padding of P = 6
-            const double aF0 = in ? (double)bU[v * PP + P * gq + T::f0pos(m, gq)] : 0.0;  // F0 at (m, j = gq)
-            const double dg = in ? sdg[gq + P * m] : 0.0;                                  // dgM(m, gq)
-            const double bF = in ? (double)bF1[v * PP + P * m + gq] : 0.0;                // F1 at (i = gq, m)
+            const double aF0 = in ? (double)bU[v * PP + f0at(m, gq)] : 0.0;  // F0 at (m, j = gq)
+            const double dg = in ? sdg[dgat(m, gq)] : 0.0;                    // dgM(m, gq)
+            const double bF = in ? (double)bF1[v * PP + f1at(gq, m)] : 0.0;   // F1 at (i = gq, m)
             asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                          : "+d"(c0), "+d"(c1)
                          : "d"(aF0), "d"(dg));
