@@ -92,20 +92,24 @@ struct TmaTraits {
   // (16 nodes) would leave half of its warp's lanes idle: two per one-warp
   // group.  A P = 6 element (36 nodes) on a two-warp group leaves 28 lanes
   // idle: four per five-warp group (144 of 160 lanes), measured 1.14x faster
-  // for ShallowWater FP64 and 1.12x for CompressibleIdealGas2D FP32, but
-  // 1.17x slower for CompressibleIdealGas2D FP64, whose larger tiles leave
-  // room for three groups only; that case keeps one element per group.
-  static constexpr int EPG = (P == 4) ? 2 : ((P == 6 && !(NV == 4 && sizeof(R) == 8)) ? 4 : 1);
+  // for ShallowWater FP64, 1.12x for CompressibleIdealGas2D FP32 and, with
+  // three 128-register groups (below), 1.27x for CompressibleIdealGas2D FP64.
+  static constexpr int EPG = (P == 4) ? 2 : ((P == 6) ? 4 : 1);
   static constexpr int TPE = (EPG * PP + 31) / 32 * 32;  // threads per group
   static_assert(TPE >= EPG * 4 * P, "the face phase gives each of the 4P face nodes its own thread");
   // 640 threads (five warps per scheduler at 96 registers) for P = 6 (ten
   // one-element or four four-element groups) and P = 8, up to 15 single-warp
   // groups for P <= 4 (named barriers 1..15; barrier 0 is the CTA-wide one).
-  // ShallowWater FP64 at P = 6 runs three four-element groups at 128
-  // registers instead: at 96 it spills (measured 108.5 against 113.5 us per
-  // stage on 256x256; the other P = 6 forms are faster with four groups).
+  // ShallowWater and CompressibleIdealGas2D FP64 at P = 6 run three
+  // four-element groups at 128 registers instead: at 96 they spill (measured
+  // 108.5 against 113.5 us per stage for ShallowWater on 256x256;
+  // CompressibleIdealGas2D's tiles leave room for three groups only anyway:
+  // 144 us, against 183 us with one-element groups).  LinearShallowWater and
+  // the FP32 forms are faster with four groups.
   static constexpr int kMaxGroups =
-      (P <= 4) ? 15 : (P == 6 ? ((EPG == 4 && Phys::kLaggedVelocity && sizeof(R) == 8) ? 3 : 640 / TPE) : 10);
+      (P <= 4) ? 15
+               : (P == 6 ? ((EPG == 4 && (Phys::kLaggedVelocity || NV == 4) && sizeof(R) == 8) ? 3 : 640 / TPE)
+                         : 10);
   static constexpr int kThreadsMax = kMaxGroups * TPE;
   // Per-element compute arrays (bulk type), laid out for conflict-free shared
   // accesses.  A 64-bit shared access is served per half-warp: two threads of
