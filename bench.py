@@ -81,12 +81,15 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def recorded_traffic():
-    """DRAM bytes per fused-stage launch from the committed ncu summary."""
+def recorded_traffic(multistage):
+    """DRAM bytes per RK stage of the C2 stage kernel from the committed ncu
+    summary: of the multi-stage launch (all stages of a solve in one launch)
+    or of the one-stage launch."""
     path = os.path.join(ROOT, "profiles", "fused_stage_cig_c2.txt")
+    key = "traffic_bytes_per_stage_multistage:" if multistage else "traffic_bytes_per_launch:"
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
+            if line.startswith(key):
                 return float(line.split(":")[1])
     except OSError:
         pass
@@ -638,7 +641,8 @@ def measure_kernel(model, Nd, nx, form, steps, kernel="persistent"):
     geo = S.SEMQuad(interp, mesh)
     cls = {"LSW": S.LinearShallowWater, "SW": S.ShallowWater, "CIG": S.CompressibleIdealGas2D}[model]
     m = cls(mesh, geo, form={"fp64": S.FP64, "fp64_ref": S.FP64_REF, "fp32": S.FP32_BULK}[form])
-    S.lib().selfgpu_model2d_set_kernel(m._h, 1 if kernel == "persistent" else 0)
+    S.lib().selfgpu_model2d_set_kernel(m._h, 0 if kernel == "per-element" else 1)
+    S.lib().selfgpu_model2d_set_multistage(m._h, 1 if kernel == "multistage" else 0)
     X, Y = geo.x[:, 0, :, :, 0], geo.x[:, 0, :, :, 1]
     Pd = Nd + 1
     nv = 4 if model == "CIG" else 3
@@ -741,6 +745,8 @@ def e2e_through_c_abi(S, mesh, geo, q0, dt, args):
     interp = geo.interp
     h = ctypes.c_void_p()
     S.check(L.selfgpu_model2d_create(ctypes.byref(h), S.MODEL_CIG, N, NEL, S.FP64, None))
+    S.check(L.selfgpu_model2d_set_kernel(h, 0 if args.kernel == "per-element" else 1))
+    S.check(L.selfgpu_model2d_set_multistage(h, 1 if args.kernel == "multistage" else 0))
     mats = [np.asfortranarray(m) for m in (interp.dgMatrix, interp.bMatrix, interp.qWeights)]
     S.check(L.selfgpu_model2d_set_interp(h, *[m.ctypes.data_as(ctypes.c_void_p) for m in mats]))
     si = np.asfortranarray(mesh.sideInfo)
@@ -798,7 +804,8 @@ def run_engine(args, rank, world, local_rank):
     mesh = S.Mesh2D(NX, NX, periodic=(True, True), perturbation=0.02)
     geo = S.SEMQuad(interp, mesh)
     model = S.CompressibleIdealGas2D(mesh, geo, stream=stream.cuda_stream)
-    S.lib().selfgpu_model2d_set_kernel(model._h, 1 if args.kernel == "persistent" else 0)
+    S.lib().selfgpu_model2d_set_kernel(model._h, 0 if args.kernel == "per-element" else 1)
+    S.lib().selfgpu_model2d_set_multistage(model._h, 1 if args.kernel == "multistage" else 0)
     q0 = initial_state(geo.x)
     torch.cuda.synchronize()
     dt = cfl_dt(geo.CovariantArcMin(), q0[:, 2].min().item())
@@ -814,6 +821,7 @@ def run_engine(args, rank, world, local_rank):
             solve()
     stream.synchronize()
     launches0 = model.LaunchCount()
+    persistent0 = S.lib().selfgpu_model2d_persistent_launch_count(model._h)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     try:
@@ -834,16 +842,23 @@ def run_engine(args, rank, world, local_rank):
         torch.cuda.synchronize()
     R.barrier()
     ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    launches = model.LaunchCount() - launches0  # fused-stage launches (plus one trace prologue per solve)
-    persistent = S.lib().selfgpu_model2d_persistent_launch_count(model._h)
+    launches = model.LaunchCount() - launches0  # stage-kernel launches (plus one trace prologue per solve)
+    persistent = S.lib().selfgpu_model2d_persistent_launch_count(model._h) - persistent0
+    # RK stages per launch of the persistent kernel: 1, or all 3 x 200 of a
+    # solve when the multi-stage launch applies (the default for this form)
+    stages_per_launch = max(1, round(3 * STEPS_PER_SOLVE * args.steps / persistent)) if persistent else 1
     clk = clocks.summary()
     t_max = R.max_over_ranks(ms)
     value = R.aggregate_rate(DOF * STEPS_PER_SOLVE * args.steps, world, t_max / 1e3)
     stage_ms = ms / (args.steps * 3 * STEPS_PER_SOLVE)
-    per_launch = algorithmic_bytes_per_element_stage() * NEL
-    achieved = per_launch / (stage_ms / 1e3) / 1e9
+    per_stage = algorithmic_bytes_per_element_stage() * NEL
+    per_launch = per_stage * stages_per_launch
+    launch_ms = stage_ms * stages_per_launch
+    achieved = per_launch / (launch_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
-    traffic = recorded_traffic()
+    traffic = recorded_traffic(stages_per_launch > 1)
+    if traffic is not None:
+        traffic *= stages_per_launch
 
     model.CheckFinite()
     e2e_ms, h2d, d2h = e2e_through_c_abi(S, mesh, geo, q0, dt, args)
@@ -864,9 +879,11 @@ def run_engine(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind,
-                     "bytes_per_launch": per_launch, "launch_ms": stage_ms,
-                     "kernel": ("k_fused_stage_tma<8,PhysCIG,double>" if persistent else
-                                "k_fused_stage<8,PhysCIG,double>") + " (one RK stage over all elements)"},
+                     "bytes_per_launch": per_launch, "launch_ms": launch_ms, "stages_per_launch": stages_per_launch,
+                     "kernel": ("k_fused_stage_tma<8,PhysCIG,double,true> (all RK stages of a 200-step solve in "
+                                "one launch)" if stages_per_launch > 1 else
+                                ("k_fused_stage_tma<8,PhysCIG,double>" if persistent else
+                                 "k_fused_stage<8,PhysCIG,double>") + " (one RK stage over all elements)")},
         "clocks": clk,
     }
     if not args.no_forms:
@@ -894,8 +911,9 @@ def main():
                     help="run only this form's measurement and print its JSON (diagnostic mode)")
     ap.add_argument("--cpu-table", action="store_true",
                     help="print the CPU-baseline table of configs C1-C5 (oracle port) and exit")
-    ap.add_argument("--kernel", default="persistent", choices=["persistent", "per-element"],
-                    help="stage kernel: persistent bulk-copy kernel or one CTA per element group")
+    ap.add_argument("--kernel", default="multistage", choices=["persistent", "multistage", "per-element"],
+                    help="stage kernel: persistent bulk-copy kernel (one launch per RK stage, or, multistage, "
+                         "all stages of a call in one launch where that applies) or one CTA per element group")
     args = ap.parse_args()
     if args.cpu_table:
         print(json.dumps(run_cpu_table()), flush=True)

@@ -339,6 +339,20 @@ int selfgpu_model2d_set_kernel(selfgpu_model2d* m, int persistent);
  * SELFGPU_ERR_TIMEOUT from sync). */
 int selfgpu_model2d_set_multistep(selfgpu_model2d* m, int enable);
 
+/* enable = 1 (the default for the SELFGPU_FP64 and SELFGPU_FP32_BULK forms;
+ * 0 for SELFGPU_FP64_REF): selfgpu_model2d_rk3 runs all 3 nSteps RK stages in
+ * ONE cooperative launch of the persistent bulk-copy kernel (one CTA per SM)
+ * where it applies: N = 7, no closure, no halo, and a mesh that gives every
+ * consumer group three to 24 elements per stage (4 440 to 35 520 elements
+ * on 148 SMs; on larger meshes the saved per-launch costs are too small to
+ * measure).
+ * Each group runs the same elements in every stage and copies the next
+ * stage's first elements ahead across the stage boundary; a stage-end
+ * counter orders only the neighbour-trace reads (bounded waits as in
+ * set_wait_limit; SELFGPU_ERR_TIMEOUT from sync).  Results equal the
+ * stage-by-stage launches bit for bit.  Elsewhere rk3 falls back to them. */
+int selfgpu_model2d_set_multistage(selfgpu_model2d* m, int enable);
+
 /* Explicit launch configuration (what the autotuner picks): persistent 0/1
  * and the persistent kernel's consumer-group cap (0 = as many as fit). */
 int selfgpu_model2d_set_launch(selfgpu_model2d* m, int persistent, int groups);
@@ -368,8 +382,11 @@ int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, f
  * wait that runs out sets an error word, the kernel stops and returns, and the
  * next selfgpu_model2d_sync() returns SELFGPU_ERR_TIMEOUT.  set_wait_limit
  * sets the bound in SM clock cycles (default 4e9, about 2 s).  inject_stall
- * (for tests of this path) makes the next launches register one element's
- * copies without issuing them, so its consumers' wait runs out. */
+ * (for tests of this path) with enable = 1 makes the next launches register
+ * one element's copies without issuing them, so its consumers' wait runs
+ * out; with enable = 2 one group of a multi-stage launch (set_multistage)
+ * never announces the end of its stages, so the others' stage-end waits run
+ * out. */
 int selfgpu_model2d_set_wait_limit(selfgpu_model2d* m, long long cycles);
 int selfgpu_model2d_inject_stall(selfgpu_model2d* m, int enable);
 

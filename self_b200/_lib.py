@@ -50,6 +50,7 @@ _SIGS = {
     "selfgpu_model2d_autotune": (c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int),
                                          ctypes.POINTER(ctypes.c_float)]),
     "selfgpu_model2d_set_launch": (c_int, [c_void_p, c_int, c_int]),
+    "selfgpu_model2d_set_multistage": (c_int, [c_void_p, c_int]),
     "selfgpu_ensemble_create": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "selfgpu_ensemble_rk3": (c_int, [c_void_p, c_double, c_int]),
     "selfgpu_ensemble_destroy": (c_int, [c_void_p]),

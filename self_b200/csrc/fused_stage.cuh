@@ -80,7 +80,8 @@ struct StageArgs {
   // bounded waits of the persistent kernel (clock cycles) and its error word
   long long waitCycles;
   int* err;
-  int debugStarve;  // test hook: the first element of CTA 0 is registered on its mbarrier but never copied
+  int debugStarve;  // test hooks: 1 = the first element of CTA 0 is registered on its mbarrier but never
+                    // copied; 2 = (multi-stage launch) group 0 of CTA 0 never announces a stage end
   // operator matrices (Lagrange%Init): dgM(ii,i) at [ii + P*i], bM(ii,side), qw;
   // bMf holds bM rounded to float for the FP32-bulk form
   double dgM[kMaxP * kMaxP];

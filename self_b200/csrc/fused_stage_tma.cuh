@@ -64,6 +64,21 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 __device__ __forceinline__ void named_bar(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+// Bounded wait until *p >= v (acquire); false when the budget ran out.
+__device__ __forceinline__ bool wait_at_least(const unsigned* p, unsigned v, long long cycles) {
+  if (ld_acquire(p) >= v) return true;
+  const long long t0 = clock64();
+  while (true) {
+    if (ld_acquire(p) >= v) return true;
+    if (clock64() - t0 > cycles) return false;
+    __nanosleep(128);
+  }
+}
 
 // Runtime layout of one element buffer (byte offsets; -1 = piece absent) and
 // of the CTA's shared memory.  Built on the host by make_tma_plan().
@@ -74,6 +89,31 @@ struct TmaPlan {
   int oX[5];       // model fields: LSW (H, Hb, fC), SW (topoB, grad), CIG (envG, drag, presc x3 -> oX[2..4])
   int oVelOwn;
   int oMats, oFlags, oSlots, oGroups, groupBytes, smemBytes;
+};
+
+// Several RK stages in one launch of k_fused_stage_tma<..., true>: stage s
+// (0-based) is RK3 stage s % 3 with the trace and velocity caches of parity
+// cur0 + s (vcur0 + s), as selfgpu_model2d's stage-by-stage loop would issue
+// them.  Every group runs the same tiles in every stage, so each stage's own
+// data (solution, own traces and velocity traces) come from the group itself
+// and are copied ahead across the stage boundary.  Only the neighbour traces
+// need the other CTAs' stage: a group announces the end of its stage on a
+// counter (bar) and, in its next stage, its face warp waits for every
+// group's announcement before its first neighbour loads (the copies, the
+// flux phase and the divergence sums of that tile go ahead meanwhile).  One
+// face warp per tile: P = 8 (one element per group) only.  (Per-tile stage
+// flags instead of the one counter, so that no stage waits for the whole
+// grid, measured 25-45 % slower: a release fence per tile and an acquire
+// load per face thread cost more than the waits they save.)
+struct TmaSteps {
+  int nStages;
+  int nGroups;      // groups of the launch (every one has at least 3 tiles)
+  double dt;
+  double rkA[3], rkG[3];
+  void* tr[2];
+  void* vel[2];
+  int cur0, vcur0;
+  unsigned* bar;    // stage-end counter, zero at launch
 };
 
 // Smallest stride >= n values of `bytes` bytes whose byte size is 64 mod 128:
@@ -155,9 +195,9 @@ struct TmaTraits {
   }
 };
 
-template <int P, class Phys, typename R>
+template <int P, class Phys, typename R, bool kMulti = false>
 __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
-    k_fused_stage_tma(const StageArgs a, const TmaPlan pl) {
+    k_fused_stage_tma(const StageArgs a, const TmaPlan pl, const TmaSteps ms) {
   using T = TmaTraits<P, Phys, R>;
   constexpr int NV = T::NV, NT = T::NT, NF = T::NF, PP = T::PP, TS = T::TS, TPE = T::TPE, N = P - 1;
   constexpr int FS = T::FS, SS = T::SS, EPG = T::EPG, EB = T::EB;
@@ -221,10 +261,18 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   const long long nTiles = ((long long)a.nEl + EPG - 1) / EPG;
   const long long nMine =
       (long long)blockIdx.x < nTiles ? (nTiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
-  const bool rk = (a.mode == MODE_RK);
+  static_assert(!kMulti || EPG == 1, "several stages per launch: one face warp per tile");
+  const bool rk = kMulti || (a.mode == MODE_RK);
   const int g = threadIdx.x / TPE;
   const int t = threadIdx.x % TPE;
   if (g >= C) return;
+  // work items of group g: its tiles g, g + C, ... of the CTA (nMineG per
+  // stage), stage after stage
+  const long long nMineG = (long long)g < nMine ? (nMine - g + C - 1) / C : 0;
+  const long long nItems = kMulti ? nMineG * ms.nStages : nMineG;
+  auto cache_of = [&](void* const* pair, int c0, int st, const void* one) -> const void* {
+    return kMulti ? (((c0 + st) & 1) ? pair[1] : pair[0]) : one;  // a stage's input cache (no dynamic index)
+  };
 
   // Group g consumes the CTA's tiles g, g + C, g + 2C, ... through its two
   // buffers; its thread 0 issues the copies of local tile jj + 2 into the
@@ -251,23 +299,26 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     const long long r = (long long)a.nEl - e0;
     return r < EPG ? (int)r : EPG;
   };
-  auto issue = [&](long long jj) {  // thread 0 only
+  // item w = tile jj of stage st (thread 0 only)
+  auto issue = [&](long long w, int st, long long jj) {
+    if (w >= nItems) return;
     const long long k = g + jj * C;
-    if (k >= nMine) return;
-    const int buf = (int)(jj & 1);
+    const int buf = (int)(w & 1);
     const long long e = (blockIdx.x + k * gridDim.x) * EPG;  // first element of the tile
     const uint32_t nl = (EPG == 1) ? 1u : (uint32_t)tile_live(k);
     unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
     uint64_t* bar = &full[2 * g + buf];
     const uint32_t bytes = nl * (qb + gb + ob + vb + xb[0] + xb[1] + xb[2] + xb[3] + xb[4]);
     mbar_arrive_expect_tx(bar, bytes);
-    if (a.debugStarve && blockIdx.x == 0 && k == 0) return;
-    const R* trIn = reinterpret_cast<const R*>(a.trIn);
+    if (a.debugStarve == 1 && blockIdx.x == 0 && k == 0) return;
+    const R* trIn = reinterpret_cast<const R*>(cache_of(ms.tr, ms.cur0, st, a.trIn));
     bulk_g2s(sl + pl.oQ, a.q + (size_t)e * NV * PP, nl * qb, bar);
     bulk_g2s(sl + pl.oDsdx, a.geo + (size_t)e * geo_record_doubles<P>(), nl * gb, bar);
     bulk_g2s(sl + pl.oOwn, trIn + (size_t)4 * TS * e, nl * ob, bar);
     if constexpr (kSW)
-      bulk_g2s(sl + pl.oVelOwn, reinterpret_cast<const R*>(a.velIn) + (size_t)e * 8 * P, nl * vb, bar);
+      bulk_g2s(sl + pl.oVelOwn,
+               reinterpret_cast<const R*>(cache_of(ms.vel, ms.vcur0, st, a.velIn)) + (size_t)e * 8 * P, nl * vb,
+               bar);
     if constexpr (kLSW) {
       bulk_g2s(sl + pl.oX[0], a.fld[0] + (size_t)e * PP, nl * xb[0], bar);
       bulk_g2s(sl + pl.oX[1], a.fld[1] + (size_t)e * 4 * P, nl * xb[1], bar);
@@ -289,8 +340,8 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     }
   };
   if (t == 0) {
-    issue(0);
-    issue(1);
+    issue(0, 0, 0);  // (a group has at least three tiles per stage when there are several stages)
+    issue(1, 0, 1);
   }
 
   const int barId = 1 + g;
@@ -309,18 +360,37 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   R* gF1 = gU + NV * PP;        // eta flux [NV][P][P]
   R* gfb = gU + T::kU;          // [4][SS]: [NV][P] per side
   R* gD = (EPG > 1) ? gBase + EPG * EB + ee * NV * PP : gU;  // divergence sums
-  R* trOut = reinterpret_cast<R*>(a.trOut);
   constexpr int rNhat = 4 * PP * 8, rNs = rNhat + 8 * P * 8, rJ = rNs + 4 * P * 8, rSi = rJ + PP * 8;
 
-  for (long long jj = 0;; ++jj) {
+  int st = 0;        // stage of item w
+  long long jj = -1;  // index of item w's tile among the group's tiles
+  for (long long w = 0; w < nItems; ++w) {
+    if constexpr (kMulti) {
+      if (++jj == nMineG) {
+        jj = 0;
+        ++st;
+      }
+    } else {
+      jj = w;
+    }
     const long long k = g + jj * C;
-    if (k >= nMine) break;
+    // this stage's caches and RK coefficients
+    const R* trIn = reinterpret_cast<const R*>(cache_of(ms.tr, ms.cur0, st, a.trIn));
+    R* trOut = reinterpret_cast<R*>(const_cast<void*>(cache_of(ms.tr, ms.cur0, st + 1, a.trOut)));
+    const R* velIn = reinterpret_cast<const R*>(cache_of(ms.vel, ms.vcur0, st, a.velIn));
+    R* velOut = reinterpret_cast<R*>(const_cast<void*>(cache_of(ms.vel, ms.vcur0, st + 1, a.velOut)));
+    const int m3 = st % 3;
+    const double rkA = kMulti ? (m3 == 0 ? ms.rkA[0] : (m3 == 1 ? ms.rkA[1] : ms.rkA[2])) : a.rk_a;
+    const double rkG = kMulti ? (m3 == 0 ? ms.rkG[0] : (m3 == 1 ? ms.rkG[1] : ms.rkG[2])) : a.rk_g;
+    const double rkGdt = kMulti ? rkG * ms.dt : a.rk_gdt;
+    // the stage's first tile reads other CTAs' traces of the previous stage
+    const bool gridWait = kMulti && st > 0 && jj == 0;
     const long long e0 = (blockIdx.x + k * gridDim.x) * EPG;
     const int nLive = (EPG == 1) ? 1 : tile_live(k);
     const long long e = e0 + ee;
     const bool active = (t < EPG * PP) && (ee < nLive);
-    const int buf = (int)(jj & 1);
-    const uint32_t par = (uint32_t)((jj >> 1) & 1);
+    const int buf = (int)(w & 1);
+    const uint32_t par = (uint32_t)((w >> 1) & 1);
     const unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
     if (t == 0) gflag[g] = mbar_wait(&full[2 * g + buf], par, a.waitCycles) ? 1 : 0;
     named_bar(barId, TPE);
@@ -330,7 +400,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         // Wait (bounded) once more for this buffer's copies and for those of
         // the group's other buffer, so that none is pending when the CTA exits.
         mbar_wait(&full[2 * g + buf], par, a.waitCycles);
-        if (k + C < nMine) mbar_wait(&full[2 * g + (buf ^ 1)], (uint32_t)(((jj + 1) >> 1) & 1), a.waitCycles);
+        if (w + 1 < nItems) mbar_wait(&full[2 * g + (buf ^ 1)], (uint32_t)(((w + 1) >> 1) & 1), a.waitCycles);
       }
       break;
     }
@@ -376,19 +446,21 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       const long long nb =
           (ssi[4] == 0) ? (long long)TS * (ssi[3] / 10 - 1 + 4 * (long long)(ssi[2] - 1)) : -1;
       const int i2 = (ssi[3] % 10) ? N - ii : ii;
-      const R* nbr = reinterpret_cast<const R*>(a.trIn) + (nb < 0 ? 0 : nb);
+      // (several stages in one launch: through L2, as the SM's L1 may still
+      // hold these lines from two stages back)
+      auto ld = [](const R* x) -> R { return kMulti ? __ldcg(x) : *x; };
+      const R* nbr = trIn + (nb < 0 ? 0 : nb);
 #pragma unroll
-      for (int kf = 0; kf < NT; ++kf) X[kf] = (nb >= 0) ? nbr[i2 + P * kf] : (R)0;
+      for (int kf = 0; kf < NT; ++kf) X[kf] = (nb >= 0) ? ld(nbr + i2 + P * kf) : (R)0;
       if constexpr (kSW)
         if (nb >= 0) {
-          const R* vn = reinterpret_cast<const R*>(a.velIn) +
-                        (size_t)2 * P * (ssi[3] / 10 - 1 + 4 * (size_t)(ssi[2] - 1));
-          velR[0] = vn[i2];
-          velR[1] = vn[i2 + P];
+          const R* vn = velIn + (size_t)2 * P * (ssi[3] / 10 - 1 + 4 * (size_t)(ssi[2] - 1));
+          velR[0] = ld(vn + i2);
+          velR[1] = ld(vn + i2 + P);
         }
     };
     if constexpr (kNbrEarly)
-      if (faceOn) load_neighbour();
+      if (faceOn && !gridWait) load_neighbour();
 
     // ---- A: flux auxiliaries, contravariant flux.  The buffer stays valid
     // until the end of phase D, so the solution, J and the node auxiliaries
@@ -592,7 +664,14 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     // the neighbour's were loaded before phase A
     {
       if (faceOn) {
-        if constexpr (!kNbrEarly) load_neighbour();
+        if (gridWait) {
+          // every group has ended the previous stage (its traces are final):
+          // the face warp waits alone, the divergence warp goes on meanwhile
+          if ((t & 31) == 0 && !wait_at_least(ms.bar, (unsigned)st * (unsigned)ms.nGroups, a.waitCycles))
+            gflag[g] = 0;  // checked after phase C
+          __syncwarp();
+        }
+        if (!kNbrEarly || gridWait) load_neighbour();
         const long long eF = e0 + eC;
         const int bcid = ssi[4];
         const bool physical = (bcid != 0) && (ssi[2] == 0);
@@ -627,7 +706,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
           const R* vo = reinterpret_cast<const R*>(sl + pl.oVelOwn + (size_t)eC * vb);
           velL[0] = vo[ii + P * (0 + 2 * s1)];
           velL[1] = vo[ii + P * (1 + 2 * s1)];
-          R* vOut = reinterpret_cast<R*>(a.velOut);
+          R* vOut = velOut;
           if constexpr (ref_rounding<R>()) {
             vOut[ii + P * (0 + 2 * (s1 + 4 * eF))] = L[0] / L[2];
             vOut[ii + P * (1 + 2 * (s1 + 4 * eF))] = L[1] / L[2];
@@ -647,6 +726,13 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       }
     }
     named_bar(barId, TPE);  // flux and face values ready
+    if (gridWait && !gflag[g]) {  // the stage-end wait ran out
+      if (t == 0) {
+        if (a.err) atomicExch(a.err, 1);
+        if (w + 1 < nItems) mbar_wait(&full[2 * g + (buf ^ 1)], (uint32_t)(((w + 1) >> 1) & 1), a.waitCycles);
+      }
+      break;
+    }
 
     // ---- D: weak divergence + lift, 1/J, source, RK update
     double dsdt[NV], qv[NV], Gv[NV];
@@ -691,7 +777,8 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     named_bar(barId, TPE);  // every thread is done reading the flux arrays and the buffer
     if (t == 0) {  // refill the buffer: generic-proxy reads before the async-proxy writes
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue(jj + 2);
+      if (!kMulti || jj + 2 < nMineG) issue(w + 2, st, jj + 2);
+      else issue(w + 2, st + 1, jj + 2 - nMineG);
     }
     if (!rk) {
       if (active)
@@ -700,11 +787,11 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       continue;
     }
     if (active) {
-      const double gdt = a.dtElem ? a.rk_g * a.dtElem[e] : a.rk_gdt;
+      const double gdt = a.dtElem ? rkG * a.dtElem[e] : rkGdt;
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
         const size_t gi = n + (size_t)PP * (v + NV * (size_t)e);
-        const double Gn = a.rk_a * Gv[v] + dsdt[v];
+        const double Gn = rkA * Gv[v] + dsdt[v];
         a.G[gi] = Gn;
         const double qn = qv[v] + gdt * Gn;
         a.q[gi] = qn;
@@ -762,6 +849,21 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       }
     }
     // no barrier here: the next tile's post-wait barrier orders the reuse of the arrays
+    if constexpr (kMulti) {
+      // This tile's solution, traces and velocity traces are read again by
+      // bulk copies (async proxy) in the next stage: the copies of tiles 0
+      // and 1 go out during this stage's last two tiles, the others during
+      // the next stage, so a proxy fence after tiles 0, 1 and the last one
+      // orders every write before the copy that reads it.
+      if (jj <= 1 || jj == nMineG - 1) asm volatile("fence.proxy.async.global;" ::: "memory");
+      if (jj == nMineG - 1 && st + 1 < ms.nStages) {  // the group's stage ends: announce it
+        named_bar(barId, TPE);
+        if (t == 0 && !(a.debugStarve == 2 && blockIdx.x == 0 && g == 0)) {
+          __threadfence();
+          atomicAdd(ms.bar, 1u);
+        }
+      }
+    }
   }
 }
 

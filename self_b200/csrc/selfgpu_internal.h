@@ -51,6 +51,15 @@ cudaError_t launch_steps_fp64(int model, int P, const StageArgs& a, const StepsA
 cudaError_t launch_steps_fp64_ref(int model, int P, const StageArgs& a, const StepsArgs& sa, int numSMs,
                                   cudaStream_t st);
 cudaError_t launch_steps_fp32(int model, int P, const StageArgs& a, const StepsArgs& sa, int numSMs, cudaStream_t st);
+// several RK stages in one cooperative launch of the persistent kernel
+// (k_fused_stage_tma<..., true>; cudaErrorNotSupported where it does not apply)
+struct TmaSteps;
+cudaError_t launch_stages_tma_fp64(int model, int P, const StageArgs& a, const StageLaunch& L, const TmaSteps& ms,
+                                   cudaStream_t st);
+cudaError_t launch_stages_tma_fp64_ref(int model, int P, const StageArgs& a, const StageLaunch& L,
+                                       const TmaSteps& ms, cudaStream_t st);
+cudaError_t launch_stages_tma_fp32(int model, int P, const StageArgs& a, const StageLaunch& L, const TmaSteps& ms,
+                                   cudaStream_t st);
 // Artificial-viscosity closure (av_closure.cuh).
 struct AvArgs;
 // closure: the viscosity kernel and the viscous-term kernel of one stage

@@ -66,13 +66,86 @@ cudaError_t launch_one(const StageArgs& a, const StageLaunch& L, cudaStream_t st
       cfg.attrs = attr;
       cfg.numAttrs = 1;
       *usedTma = 1;
-      return cudaLaunchKernelEx(&cfg, k_fused_stage_tma<P, Phys, R>, a, pl);
+      const TmaSteps none{};
+      return cudaLaunchKernelEx(&cfg, k_fused_stage_tma<P, Phys, R>, a, pl, none);
     }
   }
   constexpr int EPB = elems_per_block<P, Phys, R>();
   const int grid = (a.nEl + EPB - 1) / EPB;
   k_fused_stage<P, Phys, R, EPB><<<grid, EPB * P * P, 0, st>>>(a);
   return cudaGetLastError();
+}
+
+// ms.nStages RK stages in one cooperative launch of the persistent kernel
+// (k_fused_stage_tma<..., true>).  cudaErrorNotSupported where it does not
+// apply (P != 8, unaligned buffers, a mesh that gives some group fewer than
+// three or more than 24 tiles per stage), cudaErrorCooperativeLaunchTooLarge when the CTAs
+// cannot all be resident; the caller then falls back to stage launches.
+template <int P, class Phys, typename R>
+cudaError_t launch_stages_tma_one(const StageArgs& a, const StageLaunch& L, TmaSteps ms, cudaStream_t st) {
+  if constexpr (TmaTraits<P, Phys, R>::EPG != 1) {
+    return cudaErrorNotSupported;
+  } else {
+    bool ok = L.allowTma && a.geo != nullptr && aligned16(a.geo) && aligned16(a.q) && aligned16(a.G) &&
+              aligned16(ms.tr[0]) && aligned16(ms.tr[1]) && (ms.vel[0] == nullptr || aligned16(ms.vel[0])) &&
+              (ms.vel[1] == nullptr || aligned16(ms.vel[1])) && a.av == 0 && a.debugStarve != 1;
+    for (int k = 0; k < 5; ++k) ok = ok && (a.fld[k] == nullptr || aligned16(a.fld[k]));
+    TmaPlan pl{};
+    if (!ok || !make_tma_plan<P, Phys, R>(a, L.smemOptin, pl, L.maxGroups)) return cudaErrorNotSupported;
+    using T = TmaTraits<P, Phys, R>;
+    const long long tiles = ((long long)a.nEl + T::EPG - 1) / T::EPG;
+    const int grid = tiles < L.numSMs ? (int)tiles : L.numSMs;
+    // every group of every CTA needs three tiles per stage (the copies of the
+    // next stage's first two tiles read what the group's earlier tiles wrote);
+    // beyond 24 per group the per-launch costs this launch saves are small
+    // against the stage (measured: 1.04x at 11 tiles per group, C2, and
+    // within +-2 % at 44) and stage launches are kept
+    if (grid < 1 || tiles / grid < 3LL * pl.groups || tiles > 24LL * pl.groups * grid) return cudaErrorNotSupported;
+    static std::atomic<unsigned long long> attrSet{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+    if (!(attrSet.load() & bit)) {
+      e = cudaFuncSetAttribute(k_fused_stage_tma<P, Phys, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               L.smemOptin);
+      if (e != cudaSuccess) return e;
+      attrSet.fetch_or(bit);
+    }
+    ms.nGroups = grid * pl.groups;
+    StageArgs aa = a;
+    aa.mode = MODE_RK;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(pl.groups * T::TPE);
+    cfg.dynamicSmemBytes = pl.smemBytes;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;  // all CTAs resident: the stage-end waits need it
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_fused_stage_tma<P, Phys, R, true>, aa, pl, ms);
+  }
+}
+
+// P = 8 only: its tiles have one face warp (the stage-end wait is that
+// warp's); at P = 4 and 6 the launch measured slower than stage launches.
+template <class Phys, typename R>
+cudaError_t launch_stages_tma_P(int P, const StageArgs& a, const StageLaunch& L, const TmaSteps& ms,
+                                cudaStream_t st) {
+  return P == 8 ? launch_stages_tma_one<8, Phys, R>(a, L, ms, st) : cudaErrorNotSupported;
+}
+
+template <typename R>
+cudaError_t launch_stages_tma_impl(int model, int P, const StageArgs& a, const StageLaunch& L, const TmaSteps& ms,
+                                   cudaStream_t st) {
+  switch (model) {
+    case SELFGPU_MODEL_LSW: return launch_stages_tma_P<PhysLSW, R>(P, a, L, ms, st);
+    case SELFGPU_MODEL_SW: return launch_stages_tma_P<PhysSW, R>(P, a, L, ms, st);
+    case SELFGPU_MODEL_CIG: return launch_stages_tma_P<PhysCIG, R>(P, a, L, ms, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 template <class Phys, typename R>

@@ -15,4 +15,8 @@ cudaError_t launch_av_prep_fp32(int P, const AvArgs& a, cudaStream_t st, int num
 cudaError_t launch_steps_fp32(int model, int P, const StageArgs& a, const StepsArgs& sa, int numSMs, cudaStream_t st) {
   return launch_steps_impl<float>(model, P, a, sa, numSMs, st);
 }
+cudaError_t launch_stages_tma_fp32(int model, int P, const StageArgs& a, const StageLaunch& L, const TmaSteps& ms,
+                                  cudaStream_t st) {
+  return launch_stages_tma_impl<float>(model, P, a, L, ms, st);
+}
 }  // namespace selfgpu

@@ -55,4 +55,8 @@ cudaError_t launch_closure_features(const double* q, int P, int nEl, const AvArg
 cudaError_t launch_steps_fp64_ref(int model, int P, const StageArgs& a, const StepsArgs& sa, int numSMs, cudaStream_t st) {
   return launch_steps_impl<double>(model, P, a, sa, numSMs, st);
 }
+cudaError_t launch_stages_tma_fp64_ref(int model, int P, const StageArgs& a, const StageLaunch& L, const TmaSteps& ms,
+                                      cudaStream_t st) {
+  return launch_stages_tma_impl<double>(model, P, a, L, ms, st);
+}
 }  // namespace selfgpu

@@ -594,3 +594,97 @@ def test_one_launch_falls_back_on_a_mesh_larger_than_one_wave():
         mod.Sync()
         outs.append(mod.solution.clone())
     assert torch.equal(outs[0], outs[1])
+
+
+def _multistage_pair(model, walls, form, nx=72, N=7):
+    """Two identical handles on an nx x nx mesh (N = 7: one element per
+    group, at least three per group and stage from 4 440 elements), the first
+    with multi-stage launches on."""
+    import self_b200 as S
+    L = S.lib()
+    kw = dict(bcid=S.BC_NONORMALFLOW) if walls else dict(periodic=(True, True), perturbation=0.02)
+    out = []
+    for multi in (1, 0):
+        interp = S.Lagrange(N)
+        mesh = S.Mesh2D(nx, nx, **kw)
+        geo = S.SEMQuad(interp, mesh)
+        cls = {"LSW": S.LinearShallowWater, "SW": S.ShallowWater, "CIG": S.CompressibleIdealGas2D}[model]
+        m = cls(mesh, geo, form=form)
+        X, Y = geo.x[:, 0, :, :, 0], geo.x[:, 0, :, :, 1]
+        P = N + 1
+        q = torch.zeros((mesh.nElem, 4 if model == "CIG" else 3, P, P), device="cuda", dtype=torch.float64)
+        bump = 0.01 * torch.exp(-((X - 0.4) ** 2 + (Y - 0.6) ** 2) / 0.05)
+        if model == "CIG":
+            rho = 1.0 + 0.1 * torch.sin(2 * np.pi * X) * torch.sin(2 * np.pi * Y)
+            q[:, 0], q[:, 1], q[:, 2], q[:, 3] = rho * 0.5, rho * 0.3, rho, 2.5 + 0.17 * rho
+        elif model == "SW":
+            q[:, 0], q[:, 2] = 0.2 * bump, 1.0 + bump
+        else:
+            q[:, 2] = bump
+        m.SetSolution(q)
+        assert L.selfgpu_model2d_set_multistage(m._h, multi) == 0
+        assert L.selfgpu_model2d_set_wait_limit(m._h, 400_000_000) == 0  # ~0.2 s
+        out.append(m)
+    return out
+
+
+@pytest.mark.parametrize("model,walls", [("CIG", False), ("SW", True), ("LSW", True)])
+@pytest.mark.parametrize("form_name", ["FP64", "FP64_REF", "FP32_BULK"])
+def test_multistage_launch_equals_stage_launches(model, walls, form_name):
+    """All RK stages of an rk3 call in one launch of the persistent kernel
+    (elements copied ahead across stage boundaries, a stage-end counter before
+    the neighbour reads) give the stage-by-stage launches' state bit for bit,
+    over calls of several lengths."""
+    import self_b200 as S
+    L = S.lib()
+    a, b = _multistage_pair(model, walls, getattr(S, form_name))
+    dt = 2e-5 if model == "CIG" else 1e-4
+    l0 = L.selfgpu_model2d_launch_count(a._h)
+    for n in (5, 1, 3):
+        a.ForwardStep(n, dt)
+        b.ForwardStep(n, dt)
+    a.Sync()
+    b.Sync()
+    assert L.selfgpu_model2d_launch_count(a._h) - l0 == 1 + 3  # the trace prologue, then one launch per call
+    assert torch.isfinite(a.solution).all()
+    assert torch.equal(a.solution, b.solution) and torch.equal(a.workSol, b.workSol)
+
+
+def test_multistage_falls_back_where_it_does_not_apply():
+    """N = 5 (four-element tiles) and a mesh too small for three elements per
+    group: rk3 with multi-stage launches on runs the stage launches."""
+    import self_b200 as S
+    L = S.lib()
+    for model, nx, N in (("SW", 72, 5), ("CIG", 24, 7)):
+        a, b = _multistage_pair(model, True, S.FP64, nx=nx, N=N)
+        l0 = L.selfgpu_model2d_launch_count(a._h)
+        a.ForwardStep(4, 1e-4)
+        b.ForwardStep(4, 1e-4)
+        a.Sync()
+        b.Sync()
+        assert L.selfgpu_model2d_launch_count(a._h) - l0 == 1 + 12
+        assert torch.equal(a.solution, b.solution)
+
+
+def test_multistage_stage_end_wait_timeout_is_reported():
+    """One group never announces the end of its stages: every other group's
+    bounded stage-end wait runs out, sync reports SELFGPU_ERR_TIMEOUT (6), and
+    the handle runs normally afterwards."""
+    import self_b200 as S
+    L = S.lib()
+    a, _ = _multistage_pair("CIG", False, S.FP64)
+    assert L.selfgpu_model2d_set_wait_limit(a._h, 100_000_000) == 0  # ~50 ms
+    assert L.selfgpu_model2d_inject_stall(a._h, 2) == 0
+    a.ForwardStep(2, 2e-5)
+    with pytest.raises(S.SelfGpuError) as ei:
+        a.Sync()
+    assert ei.value.code == 6
+    assert L.selfgpu_model2d_inject_stall(a._h, 3) != 0
+    assert L.selfgpu_model2d_inject_stall(a._h, 0) == 0
+    q = torch.empty_like(a.solution)  # a uniform state (positive pressure)
+    for v, x in enumerate((0.5, 0.3, 1.0, 2.5)):
+        q[:, v] = x
+    a.SetSolution(q)
+    a.ForwardStep(2, 2e-5)
+    a.Sync()
+    a.CheckFinite()
