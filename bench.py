@@ -589,7 +589,9 @@ def measure_gas_ensemble(mlps, steps=100, n_instances=256):
         r.ForwardStep(2)
         torch.cuda.synchronize()
         r.reset()
+        torch.cuda.nvtx.range_push(f"gas_{name}")  # the timed steps, for profilers
         t = E.time_it(lambda: r.ForwardStep(steps))
+        torch.cuda.nvtx.range_pop()
         out[name] = {"value": dof * steps / t, "unit": "DOF-updates/s", "ms_per_rk3_step": 1e3 * t / steps}
         if hasattr(r, "tuning"):
             out[name]["autotune"] = {f"N={k}": v for k, v in r.tuning.items()}
