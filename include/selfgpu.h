@@ -262,7 +262,10 @@ int selfgpu_model2d_set_geometry(selfgpu_model2d* m, const double* dsdx, const d
 
 /* Model state (device, caller owned): solution interior (P,P,nVar,nEl) and
  * the RK register workSol of the same shape (zero it before the first step;
- * the reference never uploads it, hazard H21). */
+ * the reference never uploads it, hazard H21).  The SELFGPU_FP32_BULK form
+ * keeps its RK register in FP32 in engine memory (zeroed here and by
+ * selfgpu_model2d_invalidate) and neither reads nor writes workSol; its
+ * solution update uses each stage's FP64 register value before rounding. */
 int selfgpu_model2d_set_state(selfgpu_model2d* m, double* solution, double* workSol);
 
 /* Model-specific device fields (caller owned), by name:

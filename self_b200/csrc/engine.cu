@@ -169,6 +169,7 @@ struct selfgpu_model2d {
   __nv_bfloat16* mlpW = nullptr;
   float* mlpB = nullptr;
   double* geo = nullptr;  // packed geometry records (persistent kernel)
+  float* gf = nullptr;    // RK register of the FP32-bulk form (P,P,NV,nEl); workSol is unused then
   double* entropyBuf = nullptr;  // per-element entropy sums (nEl) and the total
   bool multistep = false;         // rk3 as one cooperative launch where the mesh fits one wave
   bool multistage = false;        // rk3 as one launch of the persistent kernel over all stages
@@ -451,7 +452,8 @@ int selfgpu_model2d_destroy(selfgpu_model2d* m) {
     if (m->vel[k]) cudaFree(m->vel[k]);
   }
   for (void* p : {(void*)m->avNu, (void*)m->avAct, (void*)m->avFallbacks, (void*)m->avH, m->avVisc, m->avVtr,
-                  (void*)m->mlpW, (void*)m->mlpB, (void*)m->geo, (void*)m->entropyBuf, (void*)m->stepBar})
+                  (void*)m->mlpW, (void*)m->mlpB, (void*)m->geo, (void*)m->entropyBuf, (void*)m->stepBar,
+                  (void*)m->gf})
     if (p) cudaFree(p);
   if (m->dflag) cudaFree(m->dflag);
   if (m->ownStream) cudaStreamDestroy(m->stream);
@@ -513,6 +515,18 @@ int selfgpu_model2d_set_state(selfgpu_model2d* m, double* solution, double* work
   if (!m || !solution || !workSol) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_set_state: null argument");
   m->base.q = solution;
   m->base.G = workSol;
+  if (m->form == SELFGPU_FP32_BULK && !m->gf) {
+    // the FP32-bulk form keeps its RK register in FP32, in engine memory
+    const size_t n = (size_t)m->P * m->P * nv_of(m->model) * m->nEl;
+    cudaError_t e = cudaMalloc(&m->gf, n * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->gf, 0, n * sizeof(float), m->stream);
+    if (e != cudaSuccess) {
+      if (m->gf) cudaFree(m->gf);
+      m->gf = nullptr;
+      return fail_cuda("selfgpu_model2d_set_state", e);
+    }
+    m->base.Gf = m->gf;
+  }
   m->haveState = true;
   m->valid = false;
   m->drop_graphs();
@@ -563,6 +577,11 @@ int selfgpu_model2d_set_params(selfgpu_model2d* m, double g, double fCori, doubl
 int selfgpu_model2d_invalidate(selfgpu_model2d* m) {
   if (!m) return set_error(SELFGPU_ERR_ARG, "selfgpu_model2d_invalidate: null handle");
   m->valid = false;
+  if (m->gf) {  // a new state: the FP32-bulk form's RK register starts from zero (as a zeroed workSol would)
+    const size_t n = (size_t)m->P * m->P * nv_of(m->model) * m->nEl;
+    cudaError_t e = cudaMemsetAsync(m->gf, 0, n * sizeof(float), m->stream);
+    if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_invalidate", e);
+  }
   return SELFGPU_OK;
 }
 
@@ -754,8 +773,12 @@ int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, f
   cudaError_t e = cudaMalloc(&scratch, 2 * n * sizeof(double));
   if (e != cudaSuccess) return fail_cuda("selfgpu_model2d_autotune", e);
   e = cudaMemcpyAsync(scratch, m->base.q, n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(scratch + n, m->base.G, n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);
+  if (e == cudaSuccess) {
+    if (m->gf)  // the FP32-bulk form's register (n floats fit the second half)
+      e = cudaMemcpyAsync(scratch + n, m->gf, n * sizeof(float), cudaMemcpyDeviceToDevice, m->stream);
+    else
+      e = cudaMemcpyAsync(scratch + n, m->base.G, n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);
+  }
   if (e != cudaSuccess) {
     cudaFree(scratch);
     return fail_cuda("selfgpu_model2d_autotune", e);
@@ -771,6 +794,7 @@ int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, f
   a.mode = MODE_RK;
   a.q = scratch;
   a.G = scratch + n;
+  if (m->gf) a.Gf = reinterpret_cast<float*>(scratch + n);
   a.rk_a = 0.0;
   a.rk_gdt = 0.0;
   a.rk_g = 0.0;

@@ -50,7 +50,8 @@ struct StageArgs {
   const int* __restrict__ sideInfo;   // (5,4,nEl)
   // state (caller owned, FP64)
   double* q;     // (P,P,NV,nEl)
-  double* G;     // (P,P,NV,nEl)
+  double* G;     // (P,P,NV,nEl) RK register (FP64 forms)
+  float* Gf;     // (P,P,NV,nEl) RK register of the FP32-bulk form (engine owned; G is then unused)
   double* dSdt;  // (P,P,NV,nEl), MODE_TENDENCY only
   // engine-owned trace cache (bulk type): per (element, side) a block of TS
   // values holding NT fields x P nodes, padded to 16 bytes
@@ -580,8 +581,11 @@ __device__ __forceinline__ void fused_stage_group(const StageArgs& a, const Stag
         if (sv.mode == MODE_TENDENCY) {
           a.dSdt[gi] = dsdt;
         } else {
-          const double Gn = sv.rk_a * a.G[gi] + dsdt;
-          a.G[gi] = Gn;
+          // the FP32-bulk form carries the RK register in FP32; the solution
+          // update below uses this stage's unrounded FP64 value
+          const double Gn = sv.rk_a * (sizeof(R) == 4 ? (double)a.Gf[gi] : a.G[gi]) + dsdt;
+          if constexpr (sizeof(R) == 4) a.Gf[gi] = (float)Gn;
+          else a.G[gi] = Gn;
           const double qn = qd[v] + (a.dtElem ? sv.rk_g * a.dtElem[e] : sv.rk_gdt) * Gn;
           a.q[gi] = qn;
           f[v] = (R)qn;

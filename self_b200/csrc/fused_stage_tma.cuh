@@ -739,7 +739,10 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     if (active) {
       if (rk) {  // RK register from global memory; the lift below hides the latency
 #pragma unroll
-        for (int v = 0; v < NV; ++v) Gv[v] = a.G[n + (size_t)PP * (v + NV * (size_t)e)];
+        for (int v = 0; v < NV; ++v) {
+          const size_t gi = n + (size_t)PP * (v + NV * (size_t)e);
+          Gv[v] = sizeof(R) == 4 ? (double)a.Gf[gi] : a.G[gi];  // FP32-bulk form: an FP32 register
+        }
       }
 #pragma unroll
       for (int v = 0; v < NV; ++v) qv[v] = sq[n + PP * v];
@@ -792,7 +795,8 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       for (int v = 0; v < NV; ++v) {
         const size_t gi = n + (size_t)PP * (v + NV * (size_t)e);
         const double Gn = rkA * Gv[v] + dsdt[v];
-        a.G[gi] = Gn;
+        if constexpr (sizeof(R) == 4) a.Gf[gi] = (float)Gn;  // the solution update uses the FP64 value
+        else a.G[gi] = Gn;
         const double qn = qv[v] + gdt * Gn;
         a.q[gi] = qn;
         f[v] = (R)qn;

@@ -32,7 +32,8 @@ cudaError_t launch_one(const StageArgs& a, const StageLaunch& L, cudaStream_t st
   *usedTma = 0;
   if constexpr (P % 2 == 0) {
     bool ok = L.allowTma && a.mode != MODE_TRACES && a.geo != nullptr && aligned16(a.geo) && aligned16(a.q) &&
-              aligned16(a.G) && aligned16(a.trIn) && (a.velIn == nullptr || aligned16(a.velIn));
+              aligned16(sizeof(R) == 4 ? (const void*)a.Gf : (const void*)a.G) && aligned16(a.trIn) &&
+              (a.velIn == nullptr || aligned16(a.velIn));
     for (int k = 0; k < 5; ++k) ok = ok && (a.fld[k] == nullptr || aligned16(a.fld[k]));
     TmaPlan pl{};
     if (ok && make_tma_plan<P, Phys, R>(a, L.smemOptin, pl, L.maxGroups)) {
@@ -86,7 +87,8 @@ cudaError_t launch_stages_tma_one(const StageArgs& a, const StageLaunch& L, TmaS
   if constexpr (TmaTraits<P, Phys, R>::EPG != 1) {
     return cudaErrorNotSupported;
   } else {
-    bool ok = L.allowTma && a.geo != nullptr && aligned16(a.geo) && aligned16(a.q) && aligned16(a.G) &&
+    bool ok = L.allowTma && a.geo != nullptr && aligned16(a.geo) && aligned16(a.q) &&
+              aligned16(sizeof(R) == 4 ? (const void*)a.Gf : (const void*)a.G) &&
               aligned16(ms.tr[0]) && aligned16(ms.tr[1]) && (ms.vel[0] == nullptr || aligned16(ms.vel[0])) &&
               (ms.vel[1] == nullptr || aligned16(ms.vel[1])) && a.av == 0 && a.debugStarve != 1;
     for (int k = 0; k < 5; ++k) ok = ok && (a.fld[k] == nullptr || aligned16(a.fld[k]));
