@@ -411,9 +411,9 @@ def _closure_variant(mesh, geo, q0, form, mode, mlp, steps, dt, dof, nvtx=None):
            "kernel": ("persistent, %d groups" % g_.value) if p_.value else "per-element"}
     if mode:
         nu, act, ind, (fb, evals) = model.ClosureState(reset=True)
-        res["active_elements_last_stage"] = int((act > 0).sum())
-        if mode == S.CLOSURE_MLP:
-            res["mlp_evaluation_fraction"] = evals / (3.0 * steps * model.nElem)
+        res["active_elements_last_step"] = int((act > 0).sum())
+        if mode == S.CLOSURE_MLP:  # the viscosity is formed once per RK step
+            res["mlp_evaluation_fraction"] = evals / (float(steps) * model.nElem)
             res["fallback_fraction_of_evaluations"] = fb / max(evals, 1)
             res["mean_abs_activation_diff_vs_indicator_last_stage"] = float((act - ind).abs().mean())
     sol = model.solution.clone()

@@ -430,7 +430,9 @@ int selfgpu_cig2d_tendency_noalloc(const double* solution, double* dSdt, const d
  * (BassiRebaySides + GradientBR, src/SELF_MappedData.f90:919-1078; the
  * Advection2D diffusive fluxes, src/models/hip/SELF_Advection2D.cpp:66-175)
  * with one viscosity per element.  With a closure set, every tendency / RK
- * stage adds div(nu_e grad q) through BR1, one extra launch per stage.
+ * stage adds div(nu_e grad q) through BR1.  nu_e is formed at the first
+ * stage of each RK step (and at every tendency evaluation) and held over the
+ * step's other two stages; the gradient is formed at every stage.
  *   mode 1: nu_e from the modal-decay indicator of the density (Persson &
  *           Peraire): a(s) ramps from 0 at s0 - kappa to 1 at s0 + kappa,
  *           s = log10 of the energy fraction in the highest modes;
@@ -451,7 +453,7 @@ int selfgpu_model2d_set_closure(selfgpu_model2d* m, int mode, double c, double s
  * weights (raw 16-bit patterns) and float biases / feature ranges, host arrays. */
 int selfgpu_model2d_set_mlp(selfgpu_model2d* m, const uint16_t* weights, const float* params);
 
-/* Copies (on the engine's stream) the last stage's element viscosity (nEl
+/* Copies (on the engine's stream) the element viscosity last formed (nEl
  * doubles), the activation applied and the indicator's activation (nEl floats
  * each; the latter written in mode 2) into caller-owned device arrays (each
  * may be NULL), and returns on the host (counts[2], may be NULL) the MLP

@@ -999,6 +999,7 @@ struct Model {
   Vec envGrad;
   // artificial-viscosity closure (CIG): 0 off, 1 modal-decay indicator, 2 element viscosity given
   int closure = 0;
+  bool avHeld = false;  // inside an RK step after its first stage: the step's element viscosity is kept
   double avC = 1.0, avS0 = 0.0, avKappa = 1.0;
   Vec modalT, avNu, avAct, avH, avAvg, avGrad, avGB, avGExt;
 
@@ -1434,7 +1435,7 @@ struct Model {
     if (kind == SW) { swBC(); swSource(); swRiemann(); swFlux(); }
     if (kind == CIG) { cigBC(); cigSource(); cigLLF(); cigFlux(); }
     if (kind == CIG && closure != 0) {
-      if (closure == 1) cigClosureViscosity();
+      if (closure == 1 && !avHeld) cigClosureViscosity();
       cigClosureGradient();
     }
     ContravariantProjection(flux.data(), geo->dsdx.data(), N, nVar, nEl);
@@ -1458,12 +1459,17 @@ struct Model {
   }
 
   // src/SELF_Model.f90:704-732, stepped by count (H15)
+  // The closure's element viscosity (closure 1) is formed at each step's
+  // first stage and held over the step's other two (the engine's closure does
+  // the same; not a reference routine).
   void RK3(int nSteps, double dt) {
     for (int s = 0; s < nSteps; ++s)
       for (int m = 0; m < 3; ++m) {
+        avHeld = m > 0;
         CalculateTendency();
         UpdateGRK3(m, dt);
       }
+    avHeld = false;
   }
 
   double Entropy() const {

@@ -8,11 +8,13 @@
 // viscosity per element instead of one diffusivity.
 //
 // With the closure on, each RK stage runs, before the stage kernel:
-//   k_av_nu     the element viscosity nu (modal-decay indicator of the
-//               density, or the closure MLP with the indicator as fallback and
-//               screen), and the list of elements with nu > 0: one lane per
-//               element for the indicator, warp-wide for the few elements
-//               that need the MLP or the wave speed;
+//   k_av_nu     (the first stage of an RK step, and a tendency evaluation;
+//               the step's other two stages keep its viscosity and list) the
+//               element viscosity nu (modal-decay indicator of the density,
+//               or the closure MLP with the indicator as fallback and screen),
+//               and the list of elements with nu > 0: one lane per element for
+//               the indicator, warp-wide for the few elements that need the
+//               MLP or the wave speed;
 //   k_av_grad   the listed elements only: the BR1 gradient of the four
 //               conservative variables from the averaged traces of the stage's
 //               trace cache, the contravariant viscous volume flux
@@ -613,8 +615,16 @@ struct QwArr {
   double w[kMaxP];
 };
 
+// formNu: form the element viscosity and the active list (the first stage of
+// an RK step, or a tendency evaluation); otherwise the viscous terms are
+// formed with the viscosity the step's first stage found.
 template <int P, typename R>
-cudaError_t launch_av_pair(const AvArgs& a, cudaStream_t st, int numSMs) {
+cudaError_t launch_av_pair(const AvArgs& a, cudaStream_t st, int numSMs, bool formNu) {
+  constexpr int EPB = av_elems_per_block<P, R>();
+  if (!formNu) {
+    k_av_grad<P, R, EPB><<<4 * numSMs, EPB * P * P, 0, st>>>(a);
+    return cudaGetLastError();
+  }
   cudaError_t e = cudaMemsetAsync(a.activeCount, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   // one wave of resident blocks, each warp striding over its share of the
@@ -630,21 +640,20 @@ cudaError_t launch_av_pair(const AvArgs& a, cudaStream_t st, int numSMs) {
   const long long cap = (long long)nuPerSM.load() * numSMs;
   const int g1 = (int)(nuBlocks < cap ? nuBlocks : cap);
   k_av_nu<P, R><<<g1, 32 * kNuWarps, 0, st>>>(a);
-  constexpr int EPB = av_elems_per_block<P, R>();
   k_av_grad<P, R, EPB><<<4 * numSMs, EPB * P * P, 0, st>>>(a);
   return cudaGetLastError();
 }
 
 template <typename R>
-cudaError_t launch_av_prep_impl(int P, const AvArgs& a, cudaStream_t st, int numSMs) {
+cudaError_t launch_av_prep_impl(int P, const AvArgs& a, cudaStream_t st, int numSMs, bool formNu) {
   switch (P) {
-    case 2: return launch_av_pair<2, R>(a, st, numSMs);
-    case 3: return launch_av_pair<3, R>(a, st, numSMs);
-    case 4: return launch_av_pair<4, R>(a, st, numSMs);
-    case 5: return launch_av_pair<5, R>(a, st, numSMs);
-    case 6: return launch_av_pair<6, R>(a, st, numSMs);
-    case 7: return launch_av_pair<7, R>(a, st, numSMs);
-    case 8: return launch_av_pair<8, R>(a, st, numSMs);
+    case 2: return launch_av_pair<2, R>(a, st, numSMs, formNu);
+    case 3: return launch_av_pair<3, R>(a, st, numSMs, formNu);
+    case 4: return launch_av_pair<4, R>(a, st, numSMs, formNu);
+    case 5: return launch_av_pair<5, R>(a, st, numSMs, formNu);
+    case 6: return launch_av_pair<6, R>(a, st, numSMs, formNu);
+    case 7: return launch_av_pair<7, R>(a, st, numSMs, formNu);
+    case 8: return launch_av_pair<8, R>(a, st, numSMs, formNu);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -187,9 +187,11 @@ struct selfgpu_model2d {
     }
   }
 
-  // closure preparation of one stage: element viscosity, BR1 gradient, viscous
-  // volume flux and traces, from the solution and the trace cache trIn
-  cudaError_t launch_av(const void* trIn) {
+  // closure preparation of one stage: element viscosity (formNu: the first
+  // stage of an RK step and tendency evaluations; the step's other stages
+  // keep it), BR1 gradient, viscous volume flux and traces, from the
+  // solution and the trace cache trIn
+  cudaError_t launch_av(const void* trIn, bool formNu = true) {
     AvArgs x = av;
     x.nEl = nEl;
     x.q = base.q;
@@ -201,14 +203,14 @@ struct selfgpu_model2d {
     x.trIn = trIn;
     x.presc = base.fld[2];
     x.gamma = base.gamma;
-    launches += 2;
-    return form == SELFGPU_FP32_BULK ? launch_av_prep_fp32(P, x, stream, cfg.numSMs)
-                                     : launch_av_prep_fp64(P, x, stream, cfg.numSMs);
+    launches += formNu ? 2 : 1;
+    return form == SELFGPU_FP32_BULK ? launch_av_prep_fp32(P, x, stream, cfg.numSMs, formNu)
+                                     : launch_av_prep_fp64(P, x, stream, cfg.numSMs, formNu);
   }
 
-  cudaError_t launch(StageArgs a) {
+  cudaError_t launch(StageArgs a, bool formNu = true) {
     if (avMode != AV_OFF && a.mode != MODE_TRACES) {
-      cudaError_t e = launch_av(a.trIn);
+      cudaError_t e = launch_av(a.trIn, formNu);
       if (e != cudaSuccess) return e;
     }
     ++launches;
@@ -341,7 +343,7 @@ struct selfgpu_model2d {
       vcur = 1 - vcur;
     }
     cur = 1 - cur;
-    return launch(a);
+    return launch(a, m == 0);  // the closure's viscosity: once per RK step, from the step's first stage
   }
 
   // Issue the three stages of one RK step starting from the current parities.

@@ -63,8 +63,9 @@ cudaError_t launch_stages_tma_fp32(int model, int P, const StageArgs& a, const S
 // Artificial-viscosity closure (av_closure.cuh).
 struct AvArgs;
 // closure: the viscosity kernel and the viscous-term kernel of one stage
-cudaError_t launch_av_prep_fp64(int P, const AvArgs& a, cudaStream_t st, int numSMs);
-cudaError_t launch_av_prep_fp32(int P, const AvArgs& a, cudaStream_t st, int numSMs);
+// (formNu = false: the viscous-term kernel only, with the viscosity already formed)
+cudaError_t launch_av_prep_fp64(int P, const AvArgs& a, cudaStream_t st, int numSMs, bool formNu = true);
+cudaError_t launch_av_prep_fp32(int P, const AvArgs& a, cudaStream_t st, int numSMs, bool formNu = true);
 cudaError_t launch_element_size(const double* J, const double* qw, int P, int nEl, double* h, cudaStream_t st);
 cudaError_t launch_closure_features(const double* q, int P, int nEl, const AvArgs& a, float* act, float* feat,
                                     cudaStream_t st);

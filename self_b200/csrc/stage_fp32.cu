@@ -9,8 +9,8 @@ cudaError_t launch_stage_fp32(int model, int P, const StageArgs& a, const StageL
                               int* usedTma) {
   return launch_stage_impl<float>(model, P, a, L, st, usedTma);
 }
-cudaError_t launch_av_prep_fp32(int P, const AvArgs& a, cudaStream_t st, int numSMs) {
-  return launch_av_prep_impl<float>(P, a, st, numSMs);
+cudaError_t launch_av_prep_fp32(int P, const AvArgs& a, cudaStream_t st, int numSMs, bool formNu) {
+  return launch_av_prep_impl<float>(P, a, st, numSMs, formNu);
 }
 cudaError_t launch_steps_fp32(int model, int P, const StageArgs& a, const StepsArgs& sa, int numSMs, cudaStream_t st) {
   return launch_steps_impl<float>(model, P, a, sa, numSMs, st);

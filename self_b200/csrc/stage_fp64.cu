@@ -12,8 +12,8 @@ cudaError_t launch_stage_fp64_ref(int model, int P, const StageArgs& a, const St
   return launch_stage_impl<double>(model, P, a, L, st, usedTma);
 }
 
-cudaError_t launch_av_prep_fp64(int P, const AvArgs& a, cudaStream_t st, int numSMs) {
-  return launch_av_prep_impl<double>(P, a, st, numSMs);
+cudaError_t launch_av_prep_fp64(int P, const AvArgs& a, cudaStream_t st, int numSMs, bool formNu) {
+  return launch_av_prep_impl<double>(P, a, st, numSMs, formNu);
 }
 
 // h = sqrt(sum_j sum_i w_i w_j J_ij), in the oracle's summation order
