@@ -666,8 +666,8 @@ def measure_kernel(model, Nd, nx, form, steps, kernel="persistent"):
     A = {"CIG": 0, "SW": 8 * (2 * Pd * Pd + 4 * Pd), "LSW": 8 * (2 * Pd * Pd + 4 * Pd)}[model]
     w = 4 if form == "fp32" else 8
     b = w * (4 * nv * Pd * Pd + 8 * NT * Pd) + 8 * (5 * Pd * Pd + 12 * Pd) + A + 80
-    if form == "fp32":  # FP64 solution and RK register, FP32 traces
-        b = 8 * 4 * nv * Pd * Pd + 4 * 8 * NT * Pd + 8 * (5 * Pd * Pd + 12 * Pd) + A + 80
+    if form == "fp32":  # FP64 solution, FP32 RK register and traces
+        b = 8 * 2 * nv * Pd * Pd + 4 * 2 * nv * Pd * Pd + 4 * 8 * NT * Pd + 8 * (5 * Pd * Pd + 12 * Pd) + A + 80
     us = 1e3 * ms / (3 * steps)
     return {"workload": f"{model} periodic {nx}x{nx} N={Nd} {form}, {kernel} kernel, {steps} RK3 steps",
             "us_per_stage": us, "bytes_per_element_stage": b, "elements": mesh.nElem,
