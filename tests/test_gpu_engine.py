@@ -688,3 +688,21 @@ def test_multistage_stage_end_wait_timeout_is_reported():
     a.ForwardStep(2, 2e-5)
     a.Sync()
     a.CheckFinite()
+
+
+def test_multistage_launch_with_element_time_steps():
+    """Per-element time steps (the ensembles' elementDt field) in the
+    multi-stage launch: bit for bit the stage launches' result."""
+    import self_b200 as S
+    a, b = _multistage_pair("SW", True, S.FP64)
+    nEl = a.solution.shape[0]
+    dtE = 1e-4 * (1.0 + 0.5 * torch.rand(nEl, device="cuda", dtype=torch.float64,
+                                         generator=torch.Generator(device="cuda").manual_seed(3)))
+    for m in (a, b):
+        m._set_field("elementDt", dtE)
+    a.ForwardStep(4, 0.0)
+    b.ForwardStep(4, 0.0)
+    a.Sync()
+    b.Sync()
+    assert torch.isfinite(a.solution).all()
+    assert torch.equal(a.solution, b.solution)
