@@ -33,14 +33,16 @@ __global__ void k_nonfinite(const double* __restrict__ q, long long n, int* flag
     }
 }
 
-// One element's packed geometry record (geo_record_doubles<P>() doubles):
-// dsdx (4 P^2, two planes of per-node pairs), nHat (8 P), nScale (4 P), J (P^2),
-// then sideInfo's 20 ints.  invJ = 1 stores 1/J in J's place (the forms that
-// multiply by the reciprocal instead of dividing by J).
+// One element's packed geometry record (geo_record_doubles<P, jMode != 0>()
+// doubles): dsdx (4 P^2, two planes of per-node pairs), nHat (8 P), nScale
+// (4 P), then J (jMode 1, the reference-rounding form) or 1/J (jMode 2, the
+// other forms at P < 8; at P = 8 they form 1/J from dsdx: jMode 0, no slot),
+// then sideInfo's 20 ints.
 __global__ void k_pack_geometry(const double* __restrict__ dsdx, const double* __restrict__ nHat,
                                 const double* __restrict__ nScale, const double* __restrict__ J,
-                                const int* __restrict__ sideInfo, int P, int nEl, int rec, int invJ,
+                                const int* __restrict__ sideInfo, int P, int nEl, int rec, int jMode,
                                 double* __restrict__ out) {
+  const bool withJ = jMode != 0;
   const int PP = P * P;
   const long long total = (long long)rec * nEl;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
@@ -54,10 +56,10 @@ __global__ void k_pack_geometry(const double* __restrict__ dsdx, const double* _
       v = nHat[8 * P * e + w];
     } else if ((w -= 8 * P) < 4 * P) {
       v = nScale[4 * P * e + w];
-    } else if ((w -= 4 * P) < PP) {
-      v = invJ ? 1.0 / J[PP * e + w] : J[PP * e + w];
+    } else if (withJ && (w -= 4 * P) < PP) {
+      v = jMode == 2 ? 1.0 / J[PP * e + w] : J[PP * e + w];
     } else {
-      w -= PP;  // sideInfo: two ints per double slot
+      w -= withJ ? PP : 4 * P;  // sideInfo: two ints per double slot
       int2 pr = make_int2(sideInfo[20 * e + 2 * w], sideInfo[20 * e + 2 * w + 1]);
       v = __longlong_as_double(((long long)(unsigned)pr.y << 32) | (unsigned)pr.x);
     }
@@ -494,14 +496,14 @@ int selfgpu_model2d_set_geometry(selfgpu_model2d* m, const double* dsdx, const d
   // for (set-up time): the caller's arrays stay the source of truth, and a
   // caller that changes them calls set_geometry again.
   const int P = m->P;
-  const int rec = 5 * P * P + 12 * P + 10;  // geo_record_doubles<P>()
+  const int jMode = m->form == SELFGPU_FP64_REF ? 1 : (P == 8 ? 0 : 2);
+  const int rec = (jMode ? 5 : 4) * P * P + 12 * P + 10;  // geo_record_doubles<P, jMode != 0>()
   cudaError_t e = cudaSuccess;
   if (!m->geo) e = cudaMalloc(&m->geo, (size_t)rec * m->nEl * sizeof(double));
   if (e == cudaSuccess) {
     const long long total = (long long)rec * m->nEl;
     const int blocks = (int)((total + 255) / 256 < 4096 ? (total + 255) / 256 : 4096);
-    k_pack_geometry<<<blocks, 256, 0, 0>>>(dsdx, nHat, nScale, J, sideInfo_d, P, m->nEl, rec,
-                                           m->form != SELFGPU_FP64_REF, m->geo);
+    k_pack_geometry<<<blocks, 256, 0, 0>>>(dsdx, nHat, nScale, J, sideInfo_d, P, m->nEl, rec, jMode, m->geo);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(0);

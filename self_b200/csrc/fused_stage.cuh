@@ -75,8 +75,9 @@ struct StageArgs {
   const void* vtr;
   const double* avNu;  // element viscosity: elements with nu = 0 have no viscous terms
   // engine-owned packed geometry: per element one contiguous record of
-  // geo_record_doubles<P>() doubles (dsdx, nHat, nScale, J, then sideInfo as
-  // 20 ints); read by the persistent kernel with one bulk copy
+  // geo_record_doubles<P, kJ>() doubles (dsdx, nHat, nScale, J in the
+  // reference-rounding form, then sideInfo as 20 ints); read by the
+  // persistent kernel with one bulk copy
   const double* geo;
   // bounded waits of the persistent kernel (clock cycles) and its error word
   long long waitCycles;
@@ -106,10 +107,13 @@ __device__ __forceinline__ R bm_right(const StageArgs& a, int m) {
 
 // Doubles in one element's packed geometry record: dsdx (4 P^2, as two planes
 // of P^2 pairs: (dsdx11, dsdx21) of every node, then (dsdx12, dsdx22)), nHat
-// (8 P), nScale (4 P), J (P^2), sideInfo (20 ints = 10 doubles).
-template <int P>
+// (8 P), nScale (4 P), J (P^2; J in the reference-rounding form, 1/J in the
+// others, and no slot in the others at P = 8, which take 1/J as the reciprocal
+// of det(dsdx) = J -- dsdx is the adjugate of the covariant basis), sideInfo
+// (20 ints = 10 doubles).
+template <int P, bool kJ = true>
 __host__ __device__ constexpr int geo_record_doubles() {
-  return 5 * P * P + 12 * P + 10;
+  return (kJ ? 5 : 4) * P * P + 12 * P + 10;
 }
 
 // Trace-cache block size (values of the bulk type) of one (element, side).

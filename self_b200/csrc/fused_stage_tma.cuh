@@ -279,7 +279,11 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   // buffer that tile jj has just released.  Every piece of a tile is
   // contiguous in global memory (element-major arrays), so a tile is still
   // one bulk copy per piece.
-  const uint32_t qb = NV * PP * 8, gb = geo_record_doubles<P>() * 8, ob = 4 * TS * sizeof(R);
+  // the record holds J (reference roundings), 1/J (the other forms at P < 8)
+  // or neither (the other forms at P = 8, which form 1/J from dsdx: measured
+  // faster there, slower at P = 6)
+  constexpr bool kRecJ = ref_rounding<R>() || P != 8;
+  const uint32_t qb = NV * PP * 8, gb = geo_record_doubles<P, kRecJ>() * 8, ob = 4 * TS * sizeof(R);
   const uint32_t vb = kSW ? 8 * P * sizeof(R) : 0;
   uint32_t xb[5] = {0, 0, 0, 0, 0};  // per element
   if constexpr (kLSW) {
@@ -313,7 +317,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     if (a.debugStarve == 1 && blockIdx.x == 0 && k == 0) return;
     const R* trIn = reinterpret_cast<const R*>(cache_of(ms.tr, ms.cur0, st, a.trIn));
     bulk_g2s(sl + pl.oQ, a.q + (size_t)e * NV * PP, nl * qb, bar);
-    bulk_g2s(sl + pl.oDsdx, a.geo + (size_t)e * geo_record_doubles<P>(), nl * gb, bar);
+    bulk_g2s(sl + pl.oDsdx, a.geo + (size_t)e * geo_record_doubles<P, kRecJ>(), nl * gb, bar);
     bulk_g2s(sl + pl.oOwn, trIn + (size_t)4 * TS * e, nl * ob, bar);
     if constexpr (kSW)
       bulk_g2s(sl + pl.oVelOwn,
@@ -360,7 +364,8 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   R* gF1 = gU + NV * PP;        // eta flux [NV][P][P]
   R* gfb = gU + T::kU;          // [4][SS]: [NV][P] per side
   R* gD = (EPG > 1) ? gBase + EPG * EB + ee * NV * PP : gU;  // divergence sums
-  constexpr int rNhat = 4 * PP * 8, rNs = rNhat + 8 * P * 8, rJ = rNs + 4 * P * 8, rSi = rJ + PP * 8;
+  constexpr int rNhat = 4 * PP * 8, rNs = rNhat + 8 * P * 8, rJ = rNs + 4 * P * 8;
+  constexpr int rSi = kRecJ ? rJ + PP * 8 : rJ;
 
   int st = 0;        // stage of item w
   long long jj = -1;  // index of item w's tile among the group's tiles
@@ -746,8 +751,16 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       }
 #pragma unroll
       for (int v = 0; v < NV; ++v) qv[v] = sq[n + PP * v];
-      // J of the node (reference-rounding build) or 1/J (the other forms)
-      const double Jij = reinterpret_cast<const double*>(rec + rJ)[n];
+      // J of the node (reference-rounding build) or 1/J (the other forms:
+      // from the record, or at P = 8 the reciprocal of det(dsdx) = J)
+      double Jij;
+      if constexpr (kRecJ) {
+        Jij = reinterpret_cast<const double*>(rec + rJ)[n];
+      } else {
+        const double2* gp = reinterpret_cast<const double2*>(rec);
+        const double2 c1 = gp[n], c2 = gp[PP + n];
+        Jij = 1.0 / (c1.x * c2.y - c2.x * c1.y);
+      }
       // sources in FP64 in every form (well-balanced topography / gravity terms)
       double Src[NV], na[3];
       node_aux(na);
@@ -887,11 +900,11 @@ inline bool make_tma_plan(const StageArgs& a, int smemLimit, TmaPlan& pl, int ma
   };
   if (!a.geo) return false;
   pl.oQ = put(NV * PP * 8);
-  pl.oDsdx = put(geo_record_doubles<P>() * 8);  // packed records: dsdx, nHat, nScale, J, sideInfo
+  pl.oDsdx = put(geo_record_doubles<P, ref_rounding<R>() || P != 8>() * 8);  // records: dsdx, nHat, nScale, [J,] sideInfo
   pl.oNhat = pl.oDsdx + 4 * PP * 8;              // (offsets within the first element's record)
   pl.oNs = pl.oNhat + 8 * P * 8;
   pl.oJ = pl.oNs + 4 * P * 8;
-  pl.oSi = pl.oJ + PP * 8;
+  pl.oSi = pl.oJ + ((ref_rounding<R>() || P != 8) ? PP * 8 : 0);  // (no J slot in the other forms' at P = 8)
   pl.oOwn = put(4 * TS * (int)sizeof(R));
   for (int x = 0; x < 5; ++x) pl.oX[x] = -1;
   pl.oVelOwn = -1;
