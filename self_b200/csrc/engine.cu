@@ -33,37 +33,45 @@ __global__ void k_nonfinite(const double* __restrict__ q, long long n, int* flag
     }
 }
 
-// One element's packed geometry record (geo_record_doubles<P, jMode != 0>()
-// doubles): dsdx (4 P^2, two planes of per-node pairs), nHat (8 P), nScale
-// (4 P), then J (jMode 1, the reference-rounding form) or 1/J (jMode 2, the
-// other forms at P < 8; at P = 8 they form 1/J from dsdx: jMode 0, no slot),
-// then sideInfo's 20 ints.
+// One element's packed geometry record of the given GeoKind (geo_rec(P,
+// kind).bytes): dsdx (4 P^2 values, two planes of per-node pairs), nHat (8 P),
+// nScale (4 P) -- FP64, or FP32 rounded to nearest in GEO_F32 -- then J
+// (GEO_REF) or 1/J (GEO_INVJ, GEO_F32) in FP64, none in GEO_NOJ, then
+// sideInfo's 20 ints.  One thread per 32-bit word of the records.
 __global__ void k_pack_geometry(const double* __restrict__ dsdx, const double* __restrict__ nHat,
                                 const double* __restrict__ nScale, const double* __restrict__ J,
-                                const int* __restrict__ sideInfo, int P, int nEl, int rec, int jMode,
-                                double* __restrict__ out) {
-  const bool withJ = jMode != 0;
-  const int PP = P * P;
-  const long long total = (long long)rec * nEl;
+                                const int* __restrict__ sideInfo, int P, int nEl, int kind,
+                                uint32_t* __restrict__ out) {
+  const GeoRec gr = geo_rec(P, kind);
+  const int PP = P * P, words = gr.bytes / 4;
+  const long long total = (long long)words * nEl;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
-    const long long e = k / rec;
-    int w = (int)(k - e * rec);
+    const long long e = k / words;
+    const int b = 4 * (int)(k - e * words);  // byte offset within the record
     double v = 0.0;
-    if (w < 4 * PP) {  // plane w / (2 P^2), node (w mod 2 P^2) / 2, component w mod 2
-      const int pl = w / (2 * PP), r = w - pl * 2 * PP;
-      v = dsdx[4 * PP * e + 4 * (r >> 1) + 2 * pl + (r & 1)];
-    } else if ((w -= 4 * PP) < 8 * P) {
-      v = nHat[8 * P * e + w];
-    } else if ((w -= 8 * P) < 4 * P) {
-      v = nScale[4 * P * e + w];
-    } else if (withJ && (w -= 4 * P) < PP) {
-      v = jMode == 2 ? 1.0 / J[PP * e + w] : J[PP * e + w];
+    if (b < gr.oJ) {  // metric terms: value index s
+      int s = b / gr.wm;
+      if (s < 4 * PP) {  // plane s / (2 P^2), node (s mod 2 P^2) / 2, component s mod 2
+        const int pl = s / (2 * PP), r = s - pl * 2 * PP;
+        v = dsdx[4 * PP * e + 4 * (r >> 1) + 2 * pl + (r & 1)];
+      } else if ((s -= 4 * PP) < 8 * P) {
+        v = nHat[8 * P * e + s];
+      } else {
+        v = nScale[4 * P * e + s - 8 * P];
+      }
+      if (gr.wm == 4) {
+        out[k] = __float_as_uint(__double2float_rn(v));
+        continue;
+      }
+    } else if (b < gr.oSi) {
+      const int s = (b - gr.oJ) / 8;
+      v = kind == GEO_REF ? J[PP * e + s] : 1.0 / J[PP * e + s];
     } else {
-      w -= withJ ? PP : 4 * P;  // sideInfo: two ints per double slot
-      int2 pr = make_int2(sideInfo[20 * e + 2 * w], sideInfo[20 * e + 2 * w + 1]);
-      v = __longlong_as_double(((long long)(unsigned)pr.y << 32) | (unsigned)pr.x);
+      out[k] = (uint32_t)sideInfo[20 * e + (b - gr.oSi) / 4];
+      continue;
     }
-    out[k] = v;
+    const unsigned long long u = (unsigned long long)__double_as_longlong(v);
+    out[k] = (b & 4) ? (uint32_t)(u >> 32) : (uint32_t)u;  // little-endian halves of the double
   }
 }
 
@@ -496,14 +504,18 @@ int selfgpu_model2d_set_geometry(selfgpu_model2d* m, const double* dsdx, const d
   // for (set-up time): the caller's arrays stay the source of truth, and a
   // caller that changes them calls set_geometry again.
   const int P = m->P;
-  const int jMode = m->form == SELFGPU_FP64_REF ? 1 : (P == 8 ? 0 : 2);
-  const int rec = (jMode ? 5 : 4) * P * P + 12 * P + 10;  // geo_record_doubles<P, jMode != 0>()
+  // the record kind the form's stage kernel reads (geo_kind)
+  const int kind = (m->form == SELFGPU_FP32_BULK && !(m->model == SELFGPU_MODEL_SW && P == 8)) ? GEO_F32
+                   : m->form == SELFGPU_FP64_REF ? GEO_REF
+                   : (P == 8 ? GEO_NOJ : GEO_INVJ);
+  const GeoRec gr = geo_rec(P, kind);
   cudaError_t e = cudaSuccess;
-  if (!m->geo) e = cudaMalloc(&m->geo, (size_t)rec * m->nEl * sizeof(double));
+  if (!m->geo) e = cudaMalloc(&m->geo, (size_t)gr.bytes * m->nEl);
   if (e == cudaSuccess) {
-    const long long total = (long long)rec * m->nEl;
+    const long long total = (long long)(gr.bytes / 4) * m->nEl;
     const int blocks = (int)((total + 255) / 256 < 4096 ? (total + 255) / 256 : 4096);
-    k_pack_geometry<<<blocks, 256, 0, 0>>>(dsdx, nHat, nScale, J, sideInfo_d, P, m->nEl, rec, jMode, m->geo);
+    k_pack_geometry<<<blocks, 256, 0, 0>>>(dsdx, nHat, nScale, J, sideInfo_d, P, m->nEl, kind,
+                                           reinterpret_cast<uint32_t*>(m->geo));
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(0);

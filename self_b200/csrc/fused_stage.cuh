@@ -75,9 +75,8 @@ struct StageArgs {
   const void* vtr;
   const double* avNu;  // element viscosity: elements with nu = 0 have no viscous terms
   // engine-owned packed geometry: per element one contiguous record of
-  // geo_record_doubles<P, kJ>() doubles (dsdx, nHat, nScale, J in the
-  // reference-rounding form, then sideInfo as 20 ints); read by the
-  // persistent kernel with one bulk copy
+  // geo_rec(P, kind).bytes (dsdx, nHat, nScale, J or 1/J, sideInfo; the kind
+  // follows the form); read by the persistent kernel with one bulk copy
   const double* geo;
   // bounded waits of the persistent kernel (clock cycles) and its error word
   long long waitCycles;
@@ -105,15 +104,28 @@ __device__ __forceinline__ R bm_right(const StageArgs& a, int m) {
   else return a.bMf[m + P];
 }
 
-// Doubles in one element's packed geometry record: dsdx (4 P^2, as two planes
-// of P^2 pairs: (dsdx11, dsdx21) of every node, then (dsdx12, dsdx22)), nHat
-// (8 P), nScale (4 P), J (P^2; J in the reference-rounding form, 1/J in the
-// others, and no slot in the others at P = 8, which take 1/J as the reciprocal
-// of det(dsdx) = J -- dsdx is the adjugate of the covariant basis), sideInfo
-// (20 ints = 10 doubles).
-template <int P, bool kJ = true>
-__host__ __device__ constexpr int geo_record_doubles() {
-  return (kJ ? 5 : 4) * P * P + 12 * P + 10;
+// One element's packed geometry record: dsdx (4 P^2 values, as two planes of
+// P^2 pairs: (dsdx11, dsdx21) of every node, then (dsdx12, dsdx22)), nHat
+// (8 P), nScale (4 P), a J slot (P^2 doubles), sideInfo (20 ints).  Four kinds:
+//   GEO_REF   FP64 metrics, J            (reference-rounding form)
+//   GEO_INVJ  FP64 metrics, 1/J          (production FP64 at P != 8)
+//   GEO_NOJ   FP64 metrics, no J slot    (production FP64 at P = 8: the stage
+//             takes 1/J as the reciprocal of det(dsdx) = J, dsdx being the
+//             adjugate of the covariant basis)
+//   GEO_F32   FP32 metrics, FP64 1/J     (FP32 bulk: its stage rounds dsdx,
+//             nHat and nScale to FP32 before every use, so the record holds
+//             them rounded once; 1/J stays FP64)
+// Every kind is a multiple of 16 bytes for even P.
+enum GeoKind { GEO_REF = 0, GEO_INVJ = 1, GEO_NOJ = 2, GEO_F32 = 3 };
+struct GeoRec {
+  int wm;                                // bytes per metric value (8 or 4)
+  int oNhat, oNs, oJ, oSi, bytes;        // byte offsets within a record, record size
+};
+__host__ __device__ constexpr GeoRec geo_rec(int P, int kind) {
+  const int wm = kind == GEO_F32 ? 4 : 8;
+  const int oNhat = 4 * P * P * wm, oNs = oNhat + 8 * P * wm, oJ = oNs + 4 * P * wm;
+  const int oSi = oJ + (kind == GEO_NOJ ? 0 : 8 * P * P);
+  return GeoRec{wm, oNhat, oNs, oJ, oSi, oSi + 80};
 }
 
 // Trace-cache block size (values of the bulk type) of one (element, side).
@@ -130,6 +142,17 @@ __host__ __device__ constexpr int trace_side_stride() {
 //   SW   a = (dh/dx, dh/dy)        x = (topography.boundary)
 //   CIG  a = (gx, gy, Cd)          x = prescribed (rhoU,rhoV,rho,rhoE,u,v,p,rhoH,c)
 inline namespace SELFGPU_FORM_NS {
+
+// The record kind a stage kernel of bulk type R reads at P (kSWm: the
+// ShallowWater model, whose FP32 kernel at P = 8 measured 5 % slower with the
+// FP32 record and keeps the FP64 one; every other FP32 kernel was faster).
+template <int P, typename R, bool kSWm>
+__host__ __device__ constexpr int geo_kind() {
+  return (sizeof(R) == 4 && !(kSWm && P == 8)) ? GEO_F32
+         : ref_rounding<R>()                   ? GEO_REF
+         : (P == 8 ? GEO_NOJ : GEO_INVJ);
+}
+
 struct PhysLSW {
   static constexpr int NV = 3, NT = 3, NF = 3;
   static constexpr bool kLaggedVelocity = false;

@@ -279,11 +279,13 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   // buffer that tile jj has just released.  Every piece of a tile is
   // contiguous in global memory (element-major arrays), so a tile is still
   // one bulk copy per piece.
-  // the record holds J (reference roundings), 1/J (the other forms at P < 8)
-  // or neither (the other forms at P = 8, which form 1/J from dsdx: measured
-  // faster there, slower at P = 6)
-  constexpr bool kRecJ = ref_rounding<R>() || P != 8;
-  const uint32_t qb = NV * PP * 8, gb = geo_record_doubles<P, kRecJ>() * 8, ob = 4 * TS * sizeof(R);
+  // the geometry record's kind: FP32 metrics and an FP64 1/J in the FP32-bulk
+  // form; FP64 metrics with J (reference roundings), 1/J (production FP64 at
+  // P < 8) or no J slot (production FP64 at P = 8, which forms 1/J from dsdx:
+  // measured faster there, slower at P = 6)
+  constexpr int kGeo = geo_kind<P, R, Phys::kLaggedVelocity>();
+  constexpr GeoRec kRec = geo_rec(P, kGeo);
+  const uint32_t qb = NV * PP * 8, gb = kRec.bytes, ob = 4 * TS * sizeof(R);
   const uint32_t vb = kSW ? 8 * P * sizeof(R) : 0;
   uint32_t xb[5] = {0, 0, 0, 0, 0};  // per element
   if constexpr (kLSW) {
@@ -317,7 +319,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     if (a.debugStarve == 1 && blockIdx.x == 0 && k == 0) return;
     const R* trIn = reinterpret_cast<const R*>(cache_of(ms.tr, ms.cur0, st, a.trIn));
     bulk_g2s(sl + pl.oQ, a.q + (size_t)e * NV * PP, nl * qb, bar);
-    bulk_g2s(sl + pl.oDsdx, a.geo + (size_t)e * geo_record_doubles<P, kRecJ>(), nl * gb, bar);
+    bulk_g2s(sl + pl.oDsdx, reinterpret_cast<const unsigned char*>(a.geo) + (size_t)e * gb, nl * gb, bar);
     bulk_g2s(sl + pl.oOwn, trIn + (size_t)4 * TS * e, nl * ob, bar);
     if constexpr (kSW)
       bulk_g2s(sl + pl.oVelOwn,
@@ -364,8 +366,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   R* gF1 = gU + NV * PP;        // eta flux [NV][P][P]
   R* gfb = gU + T::kU;          // [4][SS]: [NV][P] per side
   R* gD = (EPG > 1) ? gBase + EPG * EB + ee * NV * PP : gU;  // divergence sums
-  constexpr int rNhat = 4 * PP * 8, rNs = rNhat + 8 * P * 8, rJ = rNs + 4 * P * 8;
-  constexpr int rSi = kRecJ ? rJ + PP * 8 : rJ;
+  constexpr int rNhat = kRec.oNhat, rNs = kRec.oNs, rJ = kRec.oJ, rSi = kRec.oSi;
 
   int st = 0;        // stage of item w
   long long jj = -1;  // index of item w's tile among the group's tiles
@@ -481,13 +482,21 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       R Fx[NV], Fy[NV];
       Phys::template flux<R>(f, na, a, Fx, Fy);
       // dsdx planes: (dsdx11, dsdx21) of every node, then (dsdx12, dsdx22)
-      const double2* gp = reinterpret_cast<const double2*>(rec);
-      const double2 c1 = gp[n], c2 = gp[PP + n];
+      R m11, m21, m12, m22;
+      if constexpr (kRec.wm == 4) {  // FP32 record: the metric terms already rounded
+        const float2* gp = reinterpret_cast<const float2*>(rec);
+        const float2 c1 = gp[n], c2 = gp[PP + n];
+        m11 = c1.x, m21 = c1.y, m12 = c2.x, m22 = c2.y;
+      } else {
+        const double2* gp = reinterpret_cast<const double2*>(rec);
+        const double2 c1 = gp[n], c2 = gp[PP + n];
+        m11 = (R)c1.x, m21 = (R)c1.y, m12 = (R)c2.x, m22 = (R)c2.y;
+      }
       R F0[NV], F1[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        F0[v] = (R)c1.x * Fx[v] + (R)c1.y * Fy[v];
-        F1[v] = (R)c2.x * Fx[v] + (R)c2.y * Fy[v];
+        F0[v] = m11 * Fx[v] + m21 * Fy[v];
+        F1[v] = m12 * Fx[v] + m22 * Fy[v];
       }
       if constexpr (NV == 4)
         if (a.av) av_volume_add<P, R>(a, n, e, F0, F1);
@@ -684,8 +693,16 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         R L[NT];
 #pragma unroll
         for (int kf = 0; kf < NT; ++kf) L[kf] = own[ii + P * kf];
-        const double2 nh = reinterpret_cast<const double2*>(recC + rNhat)[ii + P * s1];
-        const double ns = reinterpret_cast<const double*>(recC + rNs)[ii + P * s1];
+        double2 nh;  // the face functions round the normal to R first: FP32 records hold it rounded
+        double ns;
+        if constexpr (kRec.wm == 4) {
+          const float2 nf = reinterpret_cast<const float2*>(recC + rNhat)[ii + P * s1];
+          nh = make_double2(nf.x, nf.y);
+          ns = reinterpret_cast<const float*>(recC + rNs)[ii + P * s1];
+        } else {
+          nh = reinterpret_cast<const double2*>(recC + rNhat)[ii + P * s1];
+          ns = reinterpret_cast<const double*>(recC + rNs)[ii + P * s1];
+        }
         double fx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         if constexpr (kLSW) {
           fx[0] = reinterpret_cast<const double*>(sl + pl.oX[1] + eC * xb[1])[ii + P * s1];
@@ -752,9 +769,10 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
 #pragma unroll
       for (int v = 0; v < NV; ++v) qv[v] = sq[n + PP * v];
       // J of the node (reference-rounding build) or 1/J (the other forms:
-      // from the record, or at P = 8 the reciprocal of det(dsdx) = J)
+      // from the record, or for production FP64 at P = 8 the reciprocal of
+      // det(dsdx) = J)
       double Jij;
-      if constexpr (kRecJ) {
+      if constexpr (kGeo != GEO_NOJ) {
         Jij = reinterpret_cast<const double*>(rec + rJ)[n];
       } else {
         const double2* gp = reinterpret_cast<const double2*>(rec);
@@ -779,7 +797,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         }
       } else {
         // FP32 bulk and production FP64: products with the reciprocals of the
-        // weights; the packed record of these forms holds 1/J in J's place
+        // weights, and by 1/J
         const R rwi = (R)sqwr[i], rwj = (R)sqwr[j];
         const double rJ = Jij;
 #pragma unroll
@@ -900,11 +918,12 @@ inline bool make_tma_plan(const StageArgs& a, int smemLimit, TmaPlan& pl, int ma
   };
   if (!a.geo) return false;
   pl.oQ = put(NV * PP * 8);
-  pl.oDsdx = put(geo_record_doubles<P, ref_rounding<R>() || P != 8>() * 8);  // records: dsdx, nHat, nScale, [J,] sideInfo
-  pl.oNhat = pl.oDsdx + 4 * PP * 8;              // (offsets within the first element's record)
-  pl.oNs = pl.oNhat + 8 * P * 8;
-  pl.oJ = pl.oNs + 4 * P * 8;
-  pl.oSi = pl.oJ + ((ref_rounding<R>() || P != 8) ? PP * 8 : 0);  // (no J slot in the other forms' at P = 8)
+  constexpr GeoRec gr = geo_rec(P, geo_kind<P, R, Phys::kLaggedVelocity>());
+  pl.oDsdx = put(gr.bytes);  // records: dsdx, nHat, nScale, [J or 1/J,] sideInfo
+  pl.oNhat = pl.oDsdx + gr.oNhat;  // (offsets within the first element's record)
+  pl.oNs = pl.oDsdx + gr.oNs;
+  pl.oJ = pl.oDsdx + gr.oJ;
+  pl.oSi = pl.oDsdx + gr.oSi;
   pl.oOwn = put(4 * TS * (int)sizeof(R));
   for (int x = 0; x < 5; ++x) pl.oX[x] = -1;
   pl.oVelOwn = -1;
