@@ -145,11 +145,13 @@ struct TmaTraits {
   // 108.5 against 113.5 us per stage for ShallowWater on 256x256;
   // CompressibleIdealGas2D's tiles leave room for three groups only anyway:
   // 144 us, against 183 us with one-element groups).  LinearShallowWater and
-  // the FP32 forms are faster with four groups.
+  // the FP32 forms are faster with four groups.  The FP32 forms at P = 8 run
+  // twelve groups (768 threads at 80 registers, no spills): 6-8 % faster per
+  // stage on 256x256 meshes, the same on 128x128.
   static constexpr int kMaxGroups =
       (P <= 4) ? 15
                : (P == 6 ? ((EPG == 4 && (Phys::kLaggedVelocity || NV == 4) && sizeof(R) == 8) ? 3 : 640 / TPE)
-                         : 10);
+                         : (sizeof(R) == 4 ? 12 : 10));
   static constexpr int kThreadsMax = kMaxGroups * TPE;
   // Per-element compute arrays (bulk type), laid out for conflict-free shared
   // accesses.  A 64-bit shared access is served per half-warp: two threads of
@@ -231,6 +233,9 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   double* sb = sdg + PP;
   double* sqw = sb + 2 * P;
   double* sqwr = sqw + P;  // 1/w (the FP32-bulk and production FP64 forms)
+  // bMatrix and 1/w in the bulk type (FP32-bulk form: rounded copies after 1/w)
+  R* sbR = sizeof(R) == 8 ? reinterpret_cast<R*>(sb) : reinterpret_cast<R*>(sqwr + P);
+  R* sqwrR = sizeof(R) == 8 ? reinterpret_cast<R*>(sqwr) : sbR + 2 * P;
   volatile int* gflag = reinterpret_cast<volatile int*>(smem + pl.oFlags);
   unsigned char* slots = smem + pl.oSlots;
 
@@ -242,10 +247,14 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   // where kSw8): a warp's reads of the columns of its nodes' i (or j) are then
   // consecutive
   for (int k = threadIdx.x; k < PP; k += blockDim.x) sdg[dgat(k / P, k % P)] = a.dgM[k / P + P * (k % P)];
-  for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) sb[k] = a.bM[k];
+  for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) {
+    sb[k] = a.bM[k];
+    if constexpr (sizeof(R) == 4) sbR[k] = a.bMf[k];
+  }
   for (int k = threadIdx.x; k < P; k += blockDim.x) {
     sqw[k] = a.qw[k];
     sqwr[k] = 1.0 / a.qw[k];
+    if constexpr (sizeof(R) == 4) sqwrR[k] = (R)(1.0 / a.qw[k]);
   }
   __syncthreads();
   // Launched as a programmatic dependent of the previous kernel on the stream:
@@ -798,12 +807,13 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       } else {
         // FP32 bulk and production FP64: products with the reciprocals of the
         // weights, and by 1/J
-        const R rwi = (R)sqwr[i], rwj = (R)sqwr[j];
+        const R rwi = sqwrR[i], rwj = sqwrR[j];
+        const R bi0 = sbR[i], bi1 = sbR[i + P], bj0 = sbR[j], bj1 = sbR[j + P];
         const double rJ = Jij;
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-          const R dv = d[v] + ((R)sb[i + P] * gfb[1 * SS + v * P + j] + (R)sb[i] * gfb[3 * SS + v * P + j]) * rwi +
-                       ((R)sb[j + P] * gfb[2 * SS + v * P + i] + (R)sb[j] * gfb[0 * SS + v * P + i]) * rwj;
+          const R dv = d[v] + (bi1 * gfb[1 * SS + v * P + j] + bi0 * gfb[3 * SS + v * P + j]) * rwi +
+                       (bj1 * gfb[2 * SS + v * P + i] + bj0 * gfb[0 * SS + v * P + i]) * rwj;
           dsdt[v] = Src[v] - (double)dv * rJ;
         }
       }
@@ -875,7 +885,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
 #pragma unroll
         for (int m = 0; m < P; ++m) {
           const R x = fv[row ? T::nf(fi, m, l) : T::nf(fi, l, m)];
-          lo = lo + bm_left<R>(a, m) * x;
+          lo = lo + bm_left<R>(a, m) * x;  // kernel-parameter constants (m is unrolled)
           hi = hi + bm_right<R, P>(a, m) * x;
         }
         R* o = trOut + (size_t)4 * TS * (e0 + eE);
@@ -950,6 +960,7 @@ inline bool make_tma_plan(const StageArgs& a, int smemLimit, TmaPlan& pl, int ma
     s = (s + 15) / 16 * 16;
     const int oMats = s;
     s += (PP + 4 * P) * 8;  // dgMatrix, bMatrix, weights, reciprocal weights
+    if (sizeof(R) == 4) s += (3 * P * 4 + 15) / 16 * 16;  // their FP32 copies
     const int oFlags = s;
     s += C * 4;  // group flags
     s = (s + 127) / 128 * 128;
