@@ -205,3 +205,56 @@ def test_gauss_n1_keeps_the_reference_fill_from_the_output_arrays():
     x, w = O.quadrature(1, O.GAUSS)
     np.testing.assert_array_equal(x, L.controlPoints)
     np.testing.assert_array_equal(w, L.qWeights)
+
+
+def _block2d_mesh(bc):
+    """The reference's Block2D mesh (etc/mesh/Block2D, pinned above) with every
+    physical side set to `bc` (Mesh2D%ResetBoundaryConditionType)."""
+    ref = json.load(open(os.path.join(GOLD, "reference_meshes.json")))["Block2D"]
+    nx, ny, x0, x1, y0, y1 = ref["structured"]
+    return O.Mesh(nx, ny, x0, x1, y0, y1, bcid=bc)
+
+
+@pytest.mark.parametrize("bc", [O.BC_PRESCRIBED, O.BC_NONORMALFLOW])
+def test_cig_static_fluid_stays_static(bc):
+    # test/CompressibleIdealGas2D_StaticFluid.f90 (prescribed sides from the
+    # initial state) and CompressibleIdealGas2D_StaticFluid_NoNormalFlow.f90
+    # (walls): a fluid at rest on Block2D at the CLI defaults (N = 7, Gauss,
+    # dt = 5e-4, end time 0.01 = 20 steps).  The reference asserts a finite
+    # entropy; in exact arithmetic the state does not move, so the tendency is
+    # rounding noise and the entropy (CalculateEntropy, zero for a fluid at
+    # rest) is unchanged.
+    N, P = 7, 8
+    m = _block2d_mesh(bc)
+    mod = O.Model(O.CIG, N, m)
+    q = np.zeros((P, P, 4, m.nEl), order="F")
+    q[:, :, 2] = 1.0
+    q[:, :, 3] = 1.0 / 0.4  # p = 1 with gamma = 1.4
+    mod.set("solution", q)
+    if bc == O.BC_PRESCRIBED:
+        mod.set("prescribed")
+    e0 = mod.entropy()
+    assert np.abs(mod.tendency()).max() < 1e-10
+    mod.rk3(20, 5e-4)
+    s = mod.get("solution", (P, P, 4, m.nEl))
+    assert np.abs(s - q).max() < 1e-12
+    e1 = mod.entropy()
+    assert np.isfinite(e1) and abs(e1 - e0) <= 1e-12
+
+
+def test_cig_constant_velocity_prescribed_sides():
+    # test/CompressibleIdealGas2D_ConstantVelocity.f90: a uniform flow on
+    # Block2D with the prescribed exterior state equal to it; the free stream is
+    # an exact steady solution, so the tendency is rounding noise.
+    N, P = 7, 8
+    m = _block2d_mesh(O.BC_PRESCRIBED)
+    mod = O.Model(O.CIG, N, m)
+    u, v = 0.5, 0.25
+    q = np.zeros((P, P, 4, m.nEl), order="F")
+    q[:, :, 0], q[:, :, 1], q[:, :, 2] = u, v, 1.0
+    q[:, :, 3] = 1.0 / 0.4 + 0.5 * (u * u + v * v)
+    mod.set("solution", q)
+    mod.set("prescribed")
+    assert np.abs(mod.tendency()).max() < 1e-10
+    mod.rk3(20, 5e-4)
+    assert np.abs(mod.get("solution", (P, P, 4, m.nEl)) - q).max() < 1e-11
