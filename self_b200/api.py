@@ -199,6 +199,18 @@ class Model2D:
             pass
 
     # ---- parameters and fields
+    @property
+    def g(self):
+        """Acceleration of gravity (the reference's `model % g`); assigning it
+        updates the engine's parameters."""
+        return self._g
+
+    @g.setter
+    def g(self, value):
+        self._g = float(value)
+        if getattr(self, "_h", None) is not None:
+            self._push_params()
+
     def _push_params(self):
         check(lib().selfgpu_model2d_set_params(self._h, self.g, self.fCori, self.expansionFactor, self.R))
 
