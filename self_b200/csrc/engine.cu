@@ -505,7 +505,7 @@ int selfgpu_model2d_set_geometry(selfgpu_model2d* m, const double* dsdx, const d
   // caller that changes them calls set_geometry again.
   const int P = m->P;
   // the record kind the form's stage kernel reads (geo_kind)
-  const int kind = (m->form == SELFGPU_FP32_BULK && !(m->model == SELFGPU_MODEL_SW && P == 8)) ? GEO_F32
+  const int kind = m->form == SELFGPU_FP32_BULK ? GEO_F32
                    : m->form == SELFGPU_FP64_REF ? GEO_REF
                    : (P == 8 ? GEO_NOJ : GEO_INVJ);
   const GeoRec gr = geo_rec(P, kind);

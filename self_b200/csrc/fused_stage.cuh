@@ -143,12 +143,10 @@ __host__ __device__ constexpr int trace_side_stride() {
 //   CIG  a = (gx, gy, Cd)          x = prescribed (rhoU,rhoV,rho,rhoE,u,v,p,rhoH,c)
 inline namespace SELFGPU_FORM_NS {
 
-// The record kind a stage kernel of bulk type R reads at P (kSWm: the
-// ShallowWater model, whose FP32 kernel at P = 8 measured 5 % slower with the
-// FP32 record and keeps the FP64 one; every other FP32 kernel was faster).
-template <int P, typename R, bool kSWm>
+// The record kind a stage kernel of bulk type R reads at P.
+template <int P, typename R>
 __host__ __device__ constexpr int geo_kind() {
-  return (sizeof(R) == 4 && !(kSWm && P == 8)) ? GEO_F32
+  return (sizeof(R) == 4) ? GEO_F32
          : ref_rounding<R>()                   ? GEO_REF
          : (P == 8 ? GEO_NOJ : GEO_INVJ);
 }

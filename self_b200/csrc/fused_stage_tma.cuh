@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   // form; FP64 metrics with J (reference roundings), 1/J (production FP64 at
   // P < 8) or no J slot (production FP64 at P = 8, which forms 1/J from dsdx:
   // measured faster there, slower at P = 6)
-  constexpr int kGeo = geo_kind<P, R, Phys::kLaggedVelocity>();
+  constexpr int kGeo = geo_kind<P, R>();
   constexpr GeoRec kRec = geo_rec(P, kGeo);
   const uint32_t qb = NV * PP * 8, gb = kRec.bytes, ob = 4 * TS * sizeof(R);
   const uint32_t vb = kSW ? 8 * P * sizeof(R) : 0;
@@ -928,7 +928,7 @@ inline bool make_tma_plan(const StageArgs& a, int smemLimit, TmaPlan& pl, int ma
   };
   if (!a.geo) return false;
   pl.oQ = put(NV * PP * 8);
-  constexpr GeoRec gr = geo_rec(P, geo_kind<P, R, Phys::kLaggedVelocity>());
+  constexpr GeoRec gr = geo_rec(P, geo_kind<P, R>());
   pl.oDsdx = put(gr.bytes);  // records: dsdx, nHat, nScale, [J or 1/J,] sideInfo
   pl.oNhat = pl.oDsdx + gr.oNhat;  // (offsets within the first element's record)
   pl.oNs = pl.oDsdx + gr.oNs;
