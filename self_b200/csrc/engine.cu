@@ -835,10 +835,10 @@ int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, f
   StageLaunch bestCfg = saved;
   // consumer groups per CTA: up to 10 two-warp groups for P >= 6 (12 at P = 8
   // in the FP32-bulk form and for the production FP64 ShallowWater models), up
-  // to 15 one-warp groups for P <= 4 (TmaTraits::kMaxGroups)
+  // to 20 one-warp groups for P <= 4 (TmaTraits::kMaxGroups)
   const bool twelve = m->P == 8 && (m->form == SELFGPU_FP32_BULK ||
                                     (m->form == SELFGPU_FP64 && m->model != SELFGPU_MODEL_CIG));
-  const int maxCand = m->P <= 4 ? 14 : (twelve ? 11 : 9);
+  const int maxCand = m->P <= 4 ? 19 : (twelve ? 11 : 9);
   for (int cand = 0; cand <= maxCand; ++cand) {
     StageLaunch c = saved;
     if (cand == 0) {

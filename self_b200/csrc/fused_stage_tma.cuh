@@ -138,8 +138,12 @@ struct TmaTraits {
   static constexpr int TPE = (EPG * PP + 31) / 32 * 32;  // threads per group
   static_assert(TPE >= EPG * 4 * P, "the face phase gives each of the 4P face nodes its own thread");
   // 640 threads (five warps per scheduler at 96 registers) for P = 6 (ten
-  // one-element or four four-element groups) and P = 8, up to 15 single-warp
-  // groups for P <= 4 (named barriers 1..15; barrier 0 is the CTA-wide one).
+  // one-element or four four-element groups) and P = 8; up to 20 single-warp
+  // groups for P <= 4, which synchronise with the warp barrier (15 for the
+  // FP64 CompressibleIdealGas2D and reference-rounding kernels, whose
+  // registers would not fit 20: 16 measured 0.6 % slower, 15 with the warp
+  // barrier 0.8 % faster than with named barriers).  Larger groups use
+  // named barriers 1..15 (barrier 0 is the CTA-wide one).
   // ShallowWater and CompressibleIdealGas2D FP64 at P = 6 run three
   // four-element groups at 128 registers instead: at 96 they spill (measured
   // 108.5 against 113.5 us per stage for ShallowWater on 256x256;
@@ -152,7 +156,7 @@ struct TmaTraits {
   // CompressibleIdealGas2D FP64 would spill and its shared memory holds ten
   // groups, the reference-rounding build would spill).
   static constexpr int kMaxGroups =
-      (P <= 4) ? 15
+      (P <= 4) ? (((NV == 4 && sizeof(R) == 8) || ref_rounding<R>()) ? 15 : 20)
                : (P == 6 ? ((EPG == 4 && (Phys::kLaggedVelocity || NV == 4) && sizeof(R) == 8) ? 3 : 640 / TPE)
                          : ((sizeof(R) == 4 || (NV == 3 && !ref_rounding<R>())) ? 12 : 10));
   static constexpr int kThreadsMax = kMaxGroups * TPE;
@@ -363,6 +367,12 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
   }
 
   const int barId = 1 + g;
+  // a one-warp group synchronises with the warp barrier (no named-barrier
+  // limit on the number of groups); larger groups use named barrier 1 + g
+  auto group_bar = [&]() {
+    if constexpr (TPE == 32) __syncwarp();
+    else named_bar(barId, TPE);
+  };
   // node phases: thread t serves node n of element ee of the tile
   const int ee = t / PP;
   const int n = t - ee * PP;
@@ -411,7 +421,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
     const uint32_t par = (uint32_t)((w >> 1) & 1);
     const unsigned char* sl = slots + (size_t)(2 * g + buf) * pl.slotBytes;
     if (t == 0) gflag[g] = mbar_wait(&full[2 * g + buf], par, a.waitCycles) ? 1 : 0;
-    named_bar(barId, TPE);
+    group_bar();
     if (!gflag[g]) {
       if (t == 0) {
         if (a.err) atomicExch(a.err, 1);
@@ -518,7 +528,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         gF1[v * PP + f1at(i, j)] = F1[v];
       }
     }
-    named_bar(barId, TPE);  // contravariant fluxes ready
+    group_bar();  // contravariant fluxes ready
 
     // ---- B (alongside the face phase C): weak-divergence volume sums, the
     // reference's order per node and variable (VectorDGDivergence_2D,
@@ -759,7 +769,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         for (int v = 0; v < NV; ++v) fb[s1 * SS + v * P + ii] = out[v];
       }
     }
-    named_bar(barId, TPE);  // flux and face values ready
+    group_bar();  // flux and face values ready
     if (gridWait && !gflag[g]) {  // the stage-end wait ran out
       if (t == 0) {
         if (a.err) atomicExch(a.err, 1);
@@ -821,7 +831,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
         }
       }
     }
-    named_bar(barId, TPE);  // every thread is done reading the flux arrays and the buffer
+    group_bar();  // every thread is done reading the flux arrays and the buffer
     if (t == 0) {  // refill the buffer: generic-proxy reads before the async-proxy writes
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       if (!kMulti || jj + 2 < nMineG) issue(w + 2, st, jj + 2);
@@ -849,7 +859,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
 #pragma unroll
       for (int v = 0; v < NF; ++v) gU[v * FS + T::nf(v, i, j)] = f[v];
     }
-    named_bar(barId, TPE);
+    group_bar();
 
     // ---- E: traces of the updated solution -> trace cache.  One task per
     // (element, field, line, orientation) reads the line's P values once and
@@ -905,7 +915,7 @@ __global__ void __launch_bounds__(TmaTraits<P, Phys, R>::kThreadsMax, 1)
       // orders every write before the copy that reads it.
       if (jj <= 1 || jj == nMineG - 1) asm volatile("fence.proxy.async.global;" ::: "memory");
       if (jj == nMineG - 1 && st + 1 < ms.nStages) {  // the group's stage ends: announce it
-        named_bar(barId, TPE);
+        group_bar();
         if (t == 0 && !(a.debugStarve == 2 && blockIdx.x == 0 && g == 0)) {
           __threadfence();
           atomicAdd(ms.bar, 1u);
