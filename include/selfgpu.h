@@ -347,9 +347,9 @@ int selfgpu_model2d_set_multistep(selfgpu_model2d* m, int enable);
  * ONE cooperative launch of the persistent bulk-copy kernel (one CTA per SM)
  * where it applies: N = 7, no closure, no halo, and a mesh that gives every
  * consumer group three to 24 elements per stage (4 440 to 35 520 elements
- * on 148 SMs, 5 328 to 42 624 where the kernel runs twelve groups: the
- * FP32-bulk form and the production FP64 ShallowWater models; on larger meshes
- * the saved per-launch costs are too small to measure).
+ * on 148 SMs for FP64 CompressibleIdealGas2D, 5 328 to 42 624 for the
+ * production FP64 ShallowWater models, 6 216 to 49 728 in the FP32-bulk form;
+ * on larger meshes the saved per-launch costs are too small to measure).
  * Each group runs the same elements in every stage and copies the next
  * stage's first elements ahead across the stage boundary; a stage-end
  * counter orders only the neighbour-trace reads (bounded waits as in

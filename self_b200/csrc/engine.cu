@@ -413,7 +413,7 @@ int selfgpu_model2d_create(selfgpu_model2d** out, int model, int N, int nEl, int
   m->nEl = nEl;
   m->form = form;
   // all stages of an rk3 call in one launch where that applies (N = 7, meshes
-  // of 4 440 to 35 520 elements, 5 328 to 42 624 for twelve-group kernels): measured 1-4 % faster per stage in these
+  // of 4 440 to 35 520 elements; 5 328 to 42 624 with twelve groups, 6 216 to 49 728 with fourteen): measured 1-4 % faster per stage in these
   // forms, and slower for some models in the reference-rounding form, which
   // keeps stage launches
   m->multistage = form != SELFGPU_FP64_REF;
@@ -833,12 +833,12 @@ int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, f
   const StageLaunch saved = m->cfg;
   float best = 1e30f;
   StageLaunch bestCfg = saved;
-  // consumer groups per CTA: up to 10 two-warp groups for P >= 6 (12 at P = 8
-  // in the FP32-bulk form and for the production FP64 ShallowWater models), up
+  // consumer groups per CTA: up to 10 two-warp groups for P >= 6 (at P = 8, 14
+  // in the FP32-bulk form, 12 for the production FP64 ShallowWater models), up
   // to 20 one-warp groups for P <= 4 (TmaTraits::kMaxGroups)
   const bool twelve = m->P == 8 && (m->form == SELFGPU_FP32_BULK ||
                                     (m->form == SELFGPU_FP64 && m->model != SELFGPU_MODEL_CIG));
-  const int maxCand = m->P <= 4 ? 19 : (twelve ? 11 : 9);
+  const int maxCand = m->P <= 4 ? 19 : (m->form == SELFGPU_FP32_BULK && m->P == 8 ? 13 : twelve ? 11 : 9);
   for (int cand = 0; cand <= maxCand; ++cand) {
     StageLaunch c = saved;
     if (cand == 0) {

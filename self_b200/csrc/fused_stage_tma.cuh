@@ -150,15 +150,17 @@ struct TmaTraits {
   // CompressibleIdealGas2D's tiles leave room for three groups only anyway:
   // 144 us, against 183 us with one-element groups).  LinearShallowWater and
   // the FP32 forms are faster with four groups.  The FP32 forms at P = 8 run
-  // twelve groups (768 threads at 80 registers, no spills): 6-8 % faster per
-  // stage on 256x256 meshes, the same on 128x128; so do the production FP64
+  // fourteen groups (896 threads at 72 registers, no spills): against ten,
+  // 7-16 % faster per stage on 256x256 meshes and 6 % on 128x128; fifteen (64
+  // registers) measured 1.5-22 % slower than fourteen.  Twelve
+  // groups (80 registers) run the production FP64
   // ShallowWater and LinearShallowWater kernels (80 registers without spills;
   // CompressibleIdealGas2D FP64 would spill and its shared memory holds ten
   // groups, the reference-rounding build would spill).
   static constexpr int kMaxGroups =
       (P <= 4) ? (((NV == 4 && sizeof(R) == 8) || ref_rounding<R>()) ? 15 : 20)
                : (P == 6 ? ((EPG == 4 && (Phys::kLaggedVelocity || NV == 4) && sizeof(R) == 8) ? 3 : 640 / TPE)
-                         : ((sizeof(R) == 4 || (NV == 3 && !ref_rounding<R>())) ? 12 : 10));
+                         : ((sizeof(R) == 4) ? 14 : (NV == 3 && !ref_rounding<R>()) ? 12 : 10));
   static constexpr int kThreadsMax = kMaxGroups * TPE;
   // Per-element compute arrays (bulk type), laid out for conflict-free shared
   // accesses.  A 64-bit shared access is served per half-warp: two threads of

@@ -596,10 +596,11 @@ def test_one_launch_falls_back_on_a_mesh_larger_than_one_wave():
     assert torch.equal(outs[0], outs[1])
 
 
-def _multistage_pair(model, walls, form, nx=76, N=7):
+def _multistage_pair(model, walls, form, nx=80, N=7):
     """Two identical handles on an nx x nx mesh (N = 7: one element per
     group, at least three per group and stage from 4 440 elements, 5 328 for
-    the kernels that run twelve groups), the first with multi-stage launches on."""
+    the kernels that run twelve groups, 6 216 for fourteen), the first with
+    multi-stage launches on."""
     import self_b200 as S
     L = S.lib()
     kw = dict(bcid=S.BC_NONORMALFLOW) if walls else dict(periodic=(True, True), perturbation=0.02)
