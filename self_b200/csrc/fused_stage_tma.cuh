@@ -149,7 +149,8 @@ struct TmaTraits {
   // 108.5 against 113.5 us per stage for ShallowWater on 256x256;
   // CompressibleIdealGas2D's tiles leave room for three groups only anyway:
   // 144 us, against 183 us with one-element groups).  LinearShallowWater and
-  // the FP32 forms are faster with four groups.  The FP32 forms at P = 8 run
+  // the FP32 forms are faster with four groups (five, at 72 registers with a
+  // few spilled words, measured 12-16 % slower in FP32).  The FP32 forms at P = 8 run
   // fourteen groups (896 threads at 72 registers, no spills): against ten,
   // 7-16 % faster per stage on 256x256 meshes and 6 % on 128x128; fifteen (64
   // registers) measured 1.5-22 % slower than fourteen.  Twelve
