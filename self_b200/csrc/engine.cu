@@ -835,10 +835,11 @@ int selfgpu_model2d_autotune(selfgpu_model2d* m, int* persistent, int* groups, f
   StageLaunch bestCfg = saved;
   // consumer groups per CTA: up to 10 two-warp groups for P >= 6 (at P = 8, 14
   // in the FP32-bulk form, 12 for the production FP64 ShallowWater models), up
-  // to 20 one-warp groups for P <= 4 (TmaTraits::kMaxGroups)
+  // to 20 one-warp groups for P <= 4, 24 in FP32 (TmaTraits::kMaxGroups)
   const bool twelve = m->P == 8 && (m->form == SELFGPU_FP32_BULK ||
                                     (m->form == SELFGPU_FP64 && m->model != SELFGPU_MODEL_CIG));
-  const int maxCand = m->P <= 4 ? 19 : (m->form == SELFGPU_FP32_BULK && m->P == 8 ? 13 : twelve ? 11 : 9);
+  const int maxCand = m->P <= 4 ? (m->form == SELFGPU_FP32_BULK ? 23 : 19)
+                                  : (m->form == SELFGPU_FP32_BULK && m->P == 8 ? 13 : twelve ? 11 : 9);
   for (int cand = 0; cand <= maxCand; ++cand) {
     StageLaunch c = saved;
     if (cand == 0) {

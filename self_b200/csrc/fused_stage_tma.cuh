@@ -139,7 +139,8 @@ struct TmaTraits {
   static_assert(TPE >= EPG * 4 * P, "the face phase gives each of the 4P face nodes its own thread");
   // 640 threads (five warps per scheduler at 96 registers) for P = 6 (ten
   // one-element or four four-element groups) and P = 8; up to 20 single-warp
-  // groups for P <= 4, which synchronise with the warp barrier (15 for the
+  // groups for P <= 4 (24 in FP32, at 80 registers: 2-6 % faster than 20),
+  // which synchronise with the warp barrier (15 for the
   // FP64 CompressibleIdealGas2D and reference-rounding kernels, whose
   // registers would not fit 20: 16 measured 0.6 % slower, 15 with the warp
   // barrier 0.8 % faster than with named barriers).  Larger groups use
@@ -159,7 +160,7 @@ struct TmaTraits {
   // CompressibleIdealGas2D FP64 would spill and its shared memory holds ten
   // groups, the reference-rounding build would spill).
   static constexpr int kMaxGroups =
-      (P <= 4) ? (((NV == 4 && sizeof(R) == 8) || ref_rounding<R>()) ? 15 : 20)
+      (P <= 4) ? (((NV == 4 && sizeof(R) == 8) || ref_rounding<R>()) ? 15 : (sizeof(R) == 4 ? 24 : 20))
                : (P == 6 ? ((EPG == 4 && (Phys::kLaggedVelocity || NV == 4) && sizeof(R) == 8) ? 3 : 640 / TPE)
                          : ((sizeof(R) == 4) ? 14 : (NV == 3 && !ref_rounding<R>()) ? 12 : 10));
   static constexpr int kThreadsMax = kMaxGroups * TPE;
